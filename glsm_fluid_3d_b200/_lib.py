@@ -1,0 +1,102 @@
+"""Loads libglsm_b200.so (built in-tree by build.py) and declares its C ABI.
+
+There is no fallback: if the CUDA library cannot be found or built, importing
+the package fails with the reason.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from . import build as _build
+
+_lib = None
+
+
+class GlsmError(RuntimeError):
+    pass
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if not os.path.exists(path) or _build.needs_build():
+        try:
+            _build.build()
+        except Exception as e:  # noqa: BLE001
+            if not os.path.exists(path):
+                raise ImportError(f"libglsm_b200.so is missing and could not be built: {e}") from e
+    L = ctypes.CDLL(path)
+    vp, i, d, f, u64 = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_float, ctypes.c_uint64
+    P = ctypes.POINTER
+    L.glsm_last_error.restype = ctypes.c_char_p
+    L.glsm_version.restype = i
+    sig = {
+        "glsm_gel_create": [i, i, i, d, d, d, i, i, P(vp)],
+        "glsm_gel_destroy": [vp],
+        "glsm_gel_info": [vp, P(ctypes.c_int64)],
+        "glsm_gel_steady_state": [vp, P(d)],
+        "glsm_gel_step_elasticity": [vp, i],
+        "glsm_gel_step_chemistry": [vp, i],
+        "glsm_gel_record_center": [vp, i],
+        "glsm_gel_series_config": [vp, i, i],
+        "glsm_gel_series_read": [vp, P(d), ctypes.c_size_t],
+        "glsm_gel_reset_quiescent": [vp],
+        "glsm_gel_fire_pulse": [vp],
+        "glsm_gel_set_anchor_z": [vp, d],
+        "glsm_gel_build_tube_mask": [vp, i, i],
+        "glsm_gel_set_active_from": [vp, i],
+        "glsm_gel_add_noise": [vp, u64, d],
+        "glsm_gel_read": [vp, i, P(d), ctypes.c_size_t],
+        "glsm_gel_write": [vp, i, P(d), ctypes.c_size_t],
+        "glsm_coupler_create": [P(vp), i, P(vp)],
+        "glsm_coupler_destroy": [vp],
+        "glsm_coupler_pack": [vp],
+        "glsm_coupler_scatter": [vp],
+        "glsm_coupler_repulsion": [vp],
+        "glsm_coupler_markers": [vp],
+        "glsm_coupler_read": [vp, i, P(f), ctypes.c_size_t],
+        "glsm_fluid_desc_default": [vp, i, i, i],
+        "glsm_fluid_create": [vp, vp, P(vp)],
+        "glsm_fluid_destroy": [vp],
+        "glsm_fluid_step_velocity": [vp, i],
+        "glsm_fluid_step_concentration": [vp, i],
+        "glsm_fluid_run": [vp, i, i],
+        "glsm_fluid_sync": [vp],
+        "glsm_fluid_read": [vp, i, P(f), ctypes.c_size_t],
+        "glsm_fluid_write": [vp, i, P(f), ctypes.c_size_t],
+        "glsm_fluid_info": [vp, P(ctypes.c_int64)],
+        "glsm_fluid_units": [vp, P(f)],
+    }
+    for name, args in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = i
+    L.glsm_gel_field_size.argtypes = [vp, i]
+    L.glsm_gel_field_size.restype = ctypes.c_size_t
+    L.glsm_gel_device_ptr.argtypes = [vp, i]
+    L.glsm_gel_device_ptr.restype = vp
+    L.glsm_coupler_stream.argtypes = [vp]
+    L.glsm_coupler_stream.restype = vp
+    _lib = L
+    return L
+
+
+def check(rc: int, what: str = ""):
+    if rc != 0:
+        msg = lib().glsm_last_error().decode(errors="replace")
+        raise GlsmError(f"{what}: status {rc}: {msg}")
+
+
+class FluidDesc(ctypes.Structure):
+    """glsm_fluid_desc (include/glsm_b200.h)."""
+
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int), ("nz", ctypes.c_int),
+        ("nsub", ctypes.c_int), ("storage", ctypes.c_int),
+        ("tau", ctypes.c_float), ("beta", ctypes.c_float), ("ramp_steps", ctypes.c_float),
+        ("force", ctypes.c_float * 3), ("periodic", ctypes.c_int * 3),
+        ("fp16_scale", ctypes.c_float), ("h", ctypes.c_float),
+    ]

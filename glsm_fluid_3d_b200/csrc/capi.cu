@@ -1,0 +1,1100 @@
+// capi.cu -- the C ABI of libglsm_b200.so (include/glsm_b200.h): object
+// lifecycles, host-side gel initialisation, the per-method launches that the
+// reference's classes expose, and the graph-captured fused iteration.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/glsm_b200.h"
+#include "gel.h"
+#include "glsm_internal.h"
+#include "lbm.h"
+
+using namespace glsm;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local char g_err[512] = "";
+
+static int fail(int code, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define CK(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t _e = (call);                                                              \
+        if (_e != cudaSuccess)                                                                \
+            return fail(_e == cudaErrorMemoryAllocation ? GLSM_ERR_NOMEM : GLSM_ERR_CUDA,     \
+                        "%s:%d %s: %s", __FILE__, __LINE__, #call, cudaGetErrorString(_e));   \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// handle types
+// ---------------------------------------------------------------------------
+struct glsm_coupler_s;
+struct glsm_fluid_s;
+
+struct glsm_gel_s {
+    GelDev d{};                 // descriptor with device pointers (host copy)
+    GelDev* d_self = nullptr;   // device copy for launches before coupling
+    Ctl* d_ctl = nullptr;       // control block before coupling
+    void* arena = nullptr;
+    size_t bytes = 0;
+    cudaStream_t own = nullptr;
+    double* series_extra = nullptr;  // a time-series ring larger than the built-in one
+    glsm_coupler_s* coupler = nullptr;
+    int index = -1;             // position in the coupler
+};
+
+struct glsm_coupler_s {
+    std::vector<glsm_gel_s*> gels;
+    GelDev* d_gels = nullptr;
+    MarkerDev mk{};
+    void* arena = nullptr;
+    Ctl* d_ctl = nullptr;
+    Ctl* h_ctl = nullptr;  // pinned mirror for error reads
+    cudaStream_t stream = nullptr, side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    float g2l = 1.0f, l2g = 1.0f;  // CouplerParams gel_to_lbm_vel / lbm_to_gel_vel
+    float rep_delta = 1e-4f, rep_gamma = 1.5f;  // src/coupling.cu:75-76
+    glsm_fluid_s* fluid = nullptr;
+};
+
+struct glsm_fluid_s {
+    glsm_fluid_desc desc{};
+    FluidDev F{};
+    glsm_coupler_s* c = nullptr;
+    void* arena = nullptr;
+    size_t bytes = 0;
+    unsigned* d_sync = nullptr;  // tickets[nsub], ibm_done[nsub]
+    int cur = 0;                 // current concentration buffer
+    long long substeps = 0;      // AA parity bookkeeping
+    float* scratch = nullptr;    // 19*N floats, allocated on first use
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+static size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+// carve sub-buffers out of one allocation
+struct Carver {
+    char* base;
+    size_t off = 0;
+    template <typename T>
+    T* take(size_t count) {
+        off = align_up(off, 256);
+        T* p = reinterpret_cast<T*>(base + off);
+        off += count * sizeof(T);
+        return p;
+    }
+};
+
+static uint64_t mix64(uint64_t x) {  // splitmix64 finaliser (Steele, Lea, Flood 2014)
+    uint64_t z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static double noise_unit(uint64_t seed, uint64_t gel_id, uint64_t slot, uint64_t field) {
+    const uint64_t h = mix64(mix64(mix64(seed) ^ gel_id) ^ (slot * 2ull + field));
+    return 2.0 * ((double)(h >> 11) * (1.0 / 9007199254740992.0)) - 1.0;
+}
+
+static cudaStream_t gel_stream(const glsm_gel_s* g) { return g->coupler ? g->coupler->stream : g->own; }
+
+static int upload_gel_desc(glsm_gel_s* g) {
+    CK(cudaMemcpyAsync(g->d_self, &g->d, sizeof(GelDev), cudaMemcpyHostToDevice, gel_stream(g)));
+    if (g->coupler)
+        CK(cudaMemcpyAsync(g->coupler->d_gels + g->index, &g->d, sizeof(GelDev), cudaMemcpyHostToDevice,
+                           gel_stream(g)));
+    CK(cudaStreamSynchronize(gel_stream(g)));
+    return GLSM_OK;
+}
+
+struct FieldRef {
+    void* ptr;
+    size_t count;  // doubles
+};
+static FieldRef gel_field(const glsm_gel_s* g, int field) {
+    const GelDev& d = g->d;
+    const size_t nE = d.nE, nN = d.nN;
+    switch (field) {
+        case GLSM_GEL_RN: return {d.rn, 3 * nN};
+        case GLSM_GEL_VELN: return {d.Veln, 3 * nN};
+        case GLSM_GEL_VELS: return {d.Vels, 3 * nN};
+        case GLSM_GEL_FN: return {d.Fn, 3 * nN};
+        case GLSM_GEL_UM: return {d.um, nE};
+        case GLSM_GEL_VM: return {d.vm, nE};
+        case GLSM_GEL_WM: return {d.wm, nE};
+        case GLSM_GEL_UN_NORM: return {d.un_norm, nN};
+        case GLSM_GEL_VN_NORM: return {d.vn_norm, nN};
+        case GLSM_GEL_T0: return {d.T0, nE};
+        case GLSM_GEL_T1: return {d.T1, nE};
+        case GLSM_GEL_T2: return {d.T2, nE};
+        case GLSM_GEL_RM: return {d.rm, 3 * nE};
+        case GLSM_GEL_NMSM: return {d.nmSm, 18 * nE};
+        case GLSM_GEL_VOLM: return {d.vol, nE};
+        case GLSM_GEL_PREM: return {d.pm, nE};
+        case GLSM_GEL_UN_ROBIN: return {d.un_robin, nN};
+        case GLSM_GEL_UM_NORM: return {d.um_norm, nE};
+        case GLSM_GEL_VM_NORM: return {d.vm_norm, nE};
+        case GLSM_GEL_WMP: return {d.wmp, nE};
+        case GLSM_GEL_FN_ROBIN: return {d.Fn_robin, 3 * nN};
+        case GLSM_GEL_RM_LOC: return {d.rm_loc, 24 * nE};
+        default: return {nullptr, 0};
+    }
+}
+
+// steady state of the BZ kinetics at w = FA0 by bisection on v
+// (Gel::steadyStateValue / fu_h, src/gel.cu:424-450)
+static void bz_steady_state(double f, double q, double FA0, double& u, double& v, double& w) {
+    w = FA0;
+    const double a = 1.0 - w, aa = a * a;
+    auto rate = [&](double vv) {
+        const double uu = vv / (1 - w);
+        return aa * uu - uu * uu - a * (f * vv + 0.0) * (uu - q * aa) / (uu + q * aa);
+    };
+    double hi = 1.0, lo = 0.0;
+    while (std::fabs(hi - lo) > 1e-10) {
+        const double mid = 0.5 * (hi + lo);
+        if (rate(mid) * rate(hi) < 0)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    u = lo / (1.0 - w);
+    v = lo;
+}
+
+extern "C" {
+
+const char* glsm_last_error(void) { return g_err; }
+int glsm_version(void) { return 1; }
+
+// ===========================================================================
+// Gel
+// ===========================================================================
+int glsm_gel_create(int sx, int sy, int sz, double px, double py, double pz, int gel_type, int gel_id,
+                    glsm_gel* out) {
+    if (!out || sx < 1 || sy < 1 || sz < 1 || sx > 4096 || sy > 4096 || sz > 4096)
+        return fail(GLSM_ERR_ARG, "gel size must be >= 1 element per axis");
+    if (gel_type != 1 && gel_type != 2) return fail(GLSM_ERR_ARG, "gel type must be 1 or 2");
+    auto* g = new glsm_gel_s;
+    GelDev& d = g->d;
+    d.LX = sx + 1;
+    d.LY = sy + 1;
+    d.LZ = sz + 1;
+    d.nE = (d.LX + 1) * (d.LY + 1) * (d.LZ + 1);
+    d.nN = (d.LX + 2) * (d.LY + 2) * (d.LZ + 2);
+    d.M = d.LX * d.LY * d.LZ - (d.LX - 2) * (d.LY - 2) * (d.LZ - 2);
+    d.gel_id = gel_id;
+    d.type = gel_type;
+    // GelParams defaults, src/gel.cu:630-653
+    d.f = 0.9;
+    d.ep = 0.3;
+    d.dt = 1e-3;
+    d.dtx = 5 * 1e-3;
+    d.dx = d.dy = d.dz = 1;
+    d.CH0 = 0.338;
+    d.CH1 = 0.518;
+    d.CHS = 0.1;
+    d.C0 = 1.3e-3;
+    d.AZ0 = 100.0;
+    d.FA0 = 0.139;
+    d.c0_bis = 5e-4;
+    d.b = 0.01;
+    bz_steady_state(d.f, 1e-4, d.FA0, d.uss, d.vss, d.wss);
+    d.series_every = 1000;
+    d.series_cap = 1000;
+
+    const size_t nE = d.nE, nN = d.nN;
+    size_t bytes = 0;
+    {
+        Carver cv{nullptr};
+        for (int i = 0; i < 11; i++) cv.take<double>(nE);
+        cv.take<double3>(nE);
+        cv.take<double3>(8 * nE);
+        cv.take<double3>(6 * nE);
+        for (int i = 0; i < 5; i++) cv.take<double3>(nN);
+        for (int i = 0; i < 3; i++) cv.take<double>(nN);
+        cv.take<int>(d.M);
+        cv.take<double>(12 * (size_t)d.series_cap);
+        cv.take<GelDev>(1);
+        cv.take<Ctl>(1);
+        bytes = align_up(cv.off, 256);
+    }
+    cudaError_t e = cudaMalloc(&g->arena, bytes);
+    if (e != cudaSuccess) {
+        delete g;
+        return fail(GLSM_ERR_NOMEM, "gel allocation of %zu bytes: %s", bytes, cudaGetErrorString(e));
+    }
+    g->bytes = bytes;
+    Carver cv{(char*)g->arena};
+    double** es[11] = {&d.um, &d.vm, &d.wm, &d.wmp, &d.um_norm, &d.vm_norm, &d.T0, &d.T1, &d.T2, &d.vol, &d.pm};
+    for (auto p : es) *p = cv.take<double>(nE);
+    d.rm = cv.take<double3>(nE);
+    d.rm_loc = cv.take<double3>(8 * nE);
+    d.nmSm = cv.take<double3>(6 * nE);
+    double3** ns[5] = {&d.rn, &d.Veln, &d.Vels, &d.Fn, &d.Fn_robin};
+    for (auto p : ns) *p = cv.take<double3>(nN);
+    d.un_norm = cv.take<double>(nN);
+    d.un_robin = cv.take<double>(nN);
+    d.vn_norm = cv.take<double>(nN);
+    d.bIndex = cv.take<int>(d.M);
+    d.series = cv.take<double>(12 * (size_t)d.series_cap);
+    g->d_self = cv.take<GelDev>(1);
+    g->d_ctl = cv.take<Ctl>(1);
+
+    // initial state on the host (src/gel.cu:179-219, :161-177)
+    std::vector<double> um(nE, 0.0), vm(nE, 0.0), wm(nE, 0.0);
+    for (int z = 1; z < d.LZ; z++)
+        for (int y = 1; y < d.LY; y++)
+            for (int x = 1; x < d.LX; x++) {
+                const int i = x + (d.LX + 1) * (y + (d.LY + 1) * z);
+                um[i] = d.uss;
+                vm[i] = d.vss;
+                wm[i] = d.wss;
+            }
+    const double lam = std::pow(d.FA0 / d.wss, 1 / 3.0);
+    std::vector<double3> rn(nN);
+    for (int z = 0; z < d.LZ + 2; z++)
+        for (int y = 0; y < d.LY + 2; y++)
+            for (int x = 0; x < d.LX + 2; x++) {
+                double3& r = rn[x + (d.LX + 2) * (y + (d.LY + 2) * z)];
+                r.x = px + (2 * double(x) - double(d.LX) - 1) * d.dx * lam / 2;
+                r.y = py + (2 * double(y) - double(d.LY) - 1) * d.dy * lam / 2;
+                r.z = pz + (2 * double(z) - double(d.LZ) - 1) * d.dz * lam / 2;
+            }
+    std::vector<int> surf;
+    surf.reserve(d.M);
+    for (int z = 1; z <= d.LZ; z++)
+        for (int y = 1; y <= d.LY; y++)
+            for (int x = 1; x <= d.LX; x++)
+                if (x == 1 || x == d.LX || y == 1 || y == d.LY || z == 1 || z == d.LZ)
+                    surf.push_back(x + (d.LX + 2) * (y + (d.LY + 2) * z));
+
+    e = cudaStreamCreateWithFlags(&g->own, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMemset(g->arena, 0, bytes);
+    if (e == cudaSuccess) e = cudaMemcpy(d.um, um.data(), nE * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d.vm, vm.data(), nE * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d.wm, wm.data(), nE * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d.rn, rn.data(), nN * sizeof(double3), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(d.bIndex, surf.data(), d.M * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(g->d_self, &d, sizeof(GelDev), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        if (g->own) cudaStreamDestroy(g->own);
+        cudaFree(g->arena);
+        delete g;
+        return fail(GLSM_ERR_CUDA, "gel initialisation: %s", cudaGetErrorString(e));
+    }
+    *out = g;
+    return GLSM_OK;
+}
+
+int glsm_gel_destroy(glsm_gel g) {
+    if (!g) return GLSM_OK;
+    if (g->coupler) return fail(GLSM_ERR_STATE, "destroy the coupler before its gels");
+    cudaStreamSynchronize(g->own);
+    cudaStreamDestroy(g->own);
+    if (g->series_extra) cudaFree(g->series_extra);
+    cudaFree(g->arena);
+    delete g;
+    return GLSM_OK;
+}
+
+int glsm_gel_info(glsm_gel g, int64_t out[8]) {
+    if (!g || !out) return fail(GLSM_ERR_ARG, "null argument");
+    out[0] = g->d.LX;
+    out[1] = g->d.LY;
+    out[2] = g->d.LZ;
+    out[3] = g->d.nE;
+    out[4] = g->d.nN;
+    out[5] = g->d.M;
+    out[6] = g->d.gel_id;
+    out[7] = g->d.type;
+    return GLSM_OK;
+}
+
+int glsm_gel_steady_state(glsm_gel g, double out[3]) {
+    if (!g || !out) return fail(GLSM_ERR_ARG, "null argument");
+    out[0] = g->d.uss;
+    out[1] = g->d.vss;
+    out[2] = g->d.wss;
+    return GLSM_OK;
+}
+
+static int gel_launch(glsm_gel g, int phases, int iter) {
+    if (!g) return fail(GLSM_ERR_ARG, "null gel");
+    if (iter < 0) return fail(GLSM_ERR_ARG, "iteration must be >= 0");
+    GelArgs a{};
+    if (g->coupler) {
+        a.gels = g->coupler->d_gels;
+        a.first_gel = g->index;
+        a.Mk = g->coupler->mk;
+        a.ctl = g->coupler->d_ctl;
+    } else {
+        a.gels = g->d_self;
+        a.first_gel = 0;
+        a.ctl = g->d_ctl;
+    }
+    a.phases = phases;
+    a.iter_arg = iter;
+    CK(launch_gel(a, 1, gel_stream(g)));
+    return GLSM_OK;
+}
+
+int glsm_gel_step_elasticity(glsm_gel g, int iter) { return gel_launch(g, kPhElastic, iter); }
+int glsm_gel_step_chemistry(glsm_gel g, int iter) { return gel_launch(g, kPhChem, iter); }
+int glsm_gel_record_center(glsm_gel g, int iter) { return gel_launch(g, kPhRecord, iter); }
+
+int glsm_gel_series_config(glsm_gel g, int every, int capacity) {
+    if (!g || every < 1 || capacity < 1) return fail(GLSM_ERR_ARG, "every and capacity must be >= 1");
+    if (capacity > g->d.series_cap) {
+        double* p = nullptr;
+        CK(cudaStreamSynchronize(gel_stream(g)));
+        CK(cudaMalloc(&p, 12 * sizeof(double) * (size_t)capacity));
+        CK(cudaMemset(p, 0, 12 * sizeof(double) * (size_t)capacity));
+        if (g->series_extra) cudaFree(g->series_extra);
+        g->series_extra = p;
+        g->d.series = p;
+    }
+    g->d.series_every = every;
+    g->d.series_cap = capacity;
+    return upload_gel_desc(g);
+}
+
+int glsm_gel_series_read(glsm_gel g, double* dst, size_t count) {
+    if (!g || !dst) return fail(GLSM_ERR_ARG, "null argument");
+    const size_t n = 12 * (size_t)g->d.series_cap;
+    if (count < n) return fail(GLSM_ERR_ARG, "series needs %zu doubles", n);
+    CK(cudaStreamSynchronize(gel_stream(g)));
+    CK(cudaMemcpy(dst, g->d.series, n * sizeof(double), cudaMemcpyDeviceToHost));
+    return GLSM_OK;
+}
+
+size_t glsm_gel_field_size(glsm_gel g, int field) { return g ? gel_field(g, field).count : 0; }
+
+int glsm_gel_read(glsm_gel g, int field, double* dst, size_t count) {
+    if (!g || !dst) return fail(GLSM_ERR_ARG, "null argument");
+    FieldRef f = gel_field(g, field);
+    if (!f.ptr) return fail(GLSM_ERR_ARG, "unknown gel field %d", field);
+    if (count < f.count) return fail(GLSM_ERR_ARG, "field %d needs %zu doubles", field, f.count);
+    CK(cudaMemcpyAsync(dst, f.ptr, f.count * sizeof(double), cudaMemcpyDeviceToHost, gel_stream(g)));
+    CK(cudaStreamSynchronize(gel_stream(g)));
+    return GLSM_OK;
+}
+
+int glsm_gel_write(glsm_gel g, int field, const double* src, size_t count) {
+    if (!g || !src) return fail(GLSM_ERR_ARG, "null argument");
+    FieldRef f = gel_field(g, field);
+    if (!f.ptr) return fail(GLSM_ERR_ARG, "unknown gel field %d", field);
+    if (count != f.count) return fail(GLSM_ERR_ARG, "field %d holds %zu doubles", field, f.count);
+    CK(cudaMemcpyAsync(f.ptr, src, f.count * sizeof(double), cudaMemcpyHostToDevice, gel_stream(g)));
+    CK(cudaStreamSynchronize(gel_stream(g)));
+    return GLSM_OK;
+}
+
+void* glsm_gel_device_ptr(glsm_gel g, int field) { return g ? gel_field(g, field).ptr : nullptr; }
+
+}  // extern "C"
+
+// element-slot edit on the host: read um, vm, wm, apply fn(x, y, z, u, v, w), write back
+template <typename Fn>
+static int edit_chemistry(glsm_gel g, Fn fn) {
+    const GelDev& d = g->d;
+    std::vector<double> u(d.nE), v(d.nE), w(d.nE);
+    int r;
+    if ((r = glsm_gel_read(g, GLSM_GEL_UM, u.data(), d.nE))) return r;
+    if ((r = glsm_gel_read(g, GLSM_GEL_VM, v.data(), d.nE))) return r;
+    if ((r = glsm_gel_read(g, GLSM_GEL_WM, w.data(), d.nE))) return r;
+    for (int z = 0; z <= d.LZ; z++)
+        for (int y = 0; y <= d.LY; y++)
+            for (int x = 0; x <= d.LX; x++) {
+                const int i = x + (d.LX + 1) * (y + (d.LY + 1) * z);
+                fn(x, y, z, u[i], v[i], w[i]);
+            }
+    if ((r = glsm_gel_write(g, GLSM_GEL_UM, u.data(), d.nE))) return r;
+    if ((r = glsm_gel_write(g, GLSM_GEL_VM, v.data(), d.nE))) return r;
+    return glsm_gel_write(g, GLSM_GEL_WM, w.data(), d.nE);
+}
+
+static bool host_void(const GelDev& d, int y, int z) {
+    if (d.tube_mode == 0) return false;
+    const float dy = (float)y - d.tube_cy, dz = (float)z - d.tube_cz;
+    if (d.tube_mode == 1) return std::fabs(dy) < d.tube_ihy && std::fabs(dz) < d.tube_ihz;
+    if (d.tube_ihy < 0.5f || d.tube_ihz < 0.5f) return false;
+    return (dy * dy) / (d.tube_ihy * d.tube_ihy) + (dz * dz) / (d.tube_ihz * d.tube_ihz) < 1.0f;
+}
+
+extern "C" {
+
+int glsm_gel_reset_quiescent(glsm_gel g) {
+    if (!g) return fail(GLSM_ERR_ARG, "null gel");
+    const GelDev d = g->d;
+    return edit_chemistry(g, [&](int x, int y, int z, double& u, double& v, double& w) {
+        if (x >= 1 && y >= 1 && z >= 1) {  // slots 1..LX (src/gel.cu:736-743)
+            u = d.uss * 0.01;
+            v = d.vss * 0.01;
+            w = d.wss;
+        }
+    });
+}
+
+int glsm_gel_fire_pulse(glsm_gel g) {
+    if (!g) return fail(GLSM_ERR_ARG, "null gel");
+    const GelDev d = g->d;
+    const int pw = std::max(1, d.LX / 10);
+    return edit_chemistry(g, [&](int x, int y, int z, double& u, double& v, double&) {
+        if (x >= 1 && x <= pw && y >= 1 && z >= 1 && !host_void(d, y, z)) {
+            u = d.uss * 3.0;
+            v = d.vss * 0.1;
+        }
+    });
+}
+
+int glsm_gel_set_anchor_z(glsm_gel g, double anchor_z) {
+    if (!g) return fail(GLSM_ERR_ARG, "null gel");
+    g->d.use_anchor = 1;
+    g->d.anchor_z = anchor_z;
+    return upload_gel_desc(g);
+}
+
+int glsm_gel_build_tube_mask(glsm_gel g, int wall_thickness, int circular) {
+    if (!g || wall_thickness < 0) return fail(GLSM_ERR_ARG, "bad tube mask arguments");
+    GelDev& d = g->d;
+    const float cy = (d.LY + 1) * 0.5f, cz = (d.LZ + 1) * 0.5f;
+    float ihy = (d.LY * 0.5f) - wall_thickness, ihz = (d.LZ * 0.5f) - wall_thickness;
+    if (ihy <= 0) ihy = 0;
+    if (ihz <= 0) ihz = 0;
+    d.tube_mode = circular ? 2 : 1;
+    d.tube_cy = cy;
+    d.tube_cz = cz;
+    d.tube_ihy = ihy;
+    d.tube_ihz = ihz;
+    int r = upload_gel_desc(g);
+    if (r) return r;
+    // void elements start at the steady state (src/gel.cu:835-854)
+    const GelDev dd = d;
+    return edit_chemistry(g, [&](int x, int y, int z, double& u, double& v, double& w) {
+        if (x < 1 || y < 1 || z < 1) return;
+        const float dy = (float)y - dd.tube_cy, dz = (float)z - dd.tube_cz;
+        bool vd;
+        if (circular) {
+            const float r2 = dy * dy / (dd.tube_ihy * dd.tube_ihy + 1e-6f) + dz * dz / (dd.tube_ihz * dd.tube_ihz + 1e-6f);
+            vd = dd.tube_ihy > 0 && dd.tube_ihz > 0 && r2 < 1.0f;
+        } else {
+            vd = std::fabs(dy) < dd.tube_ihy && std::fabs(dz) < dd.tube_ihz;
+        }
+        if (vd) {
+            u = dd.uss;
+            v = dd.vss;
+            w = dd.wss;
+        }
+    });
+}
+
+int glsm_gel_set_active_from(glsm_gel g, int iter) {
+    if (!g || iter < 0) return fail(GLSM_ERR_ARG, "iteration must be >= 0");
+    g->d.active_from = iter;
+    return upload_gel_desc(g);
+}
+
+int glsm_gel_add_noise(glsm_gel g, uint64_t seed, double amplitude) {
+    if (!g) return fail(GLSM_ERR_ARG, "null gel");
+    const GelDev d = g->d;
+    return edit_chemistry(g, [&](int x, int y, int z, double& u, double& v, double&) {
+        if (x >= 1 && x < d.LX && y >= 1 && y < d.LY && z >= 1 && z < d.LZ) {
+            const uint64_t slot = (uint64_t)(x + (d.LX + 1) * (y + (d.LY + 1) * z));
+            u += amplitude * noise_unit(seed, (uint64_t)d.gel_id, slot, 0);
+            v += amplitude * noise_unit(seed, (uint64_t)d.gel_id, slot, 1);
+        }
+    });
+}
+
+// ===========================================================================
+// Coupler
+// ===========================================================================
+int glsm_coupler_create(const glsm_gel* gels, int n_gels, glsm_coupler* out) {
+    if (!out || (n_gels > 0 && !gels) || n_gels < 0) return fail(GLSM_ERR_ARG, "bad gel list");
+    if (n_gels > kMaxBoxes) return fail(GLSM_ERR_ARG, "at most %d gels per coupler", kMaxBoxes);
+    for (int i = 0; i < n_gels; i++) {
+        if (!gels[i]) return fail(GLSM_ERR_ARG, "null gel %d", i);
+        if (gels[i]->coupler) return fail(GLSM_ERR_STATE, "gel %d already belongs to a coupler", i);
+        for (int j = 0; j < i; j++)
+            if (gels[j] == gels[i]) return fail(GLSM_ERR_ARG, "gel %d listed twice", i);
+    }
+    auto* c = new glsm_coupler_s;
+    int M = 0;
+    for (int i = 0; i < n_gels; i++) M += gels[i]->d.M;
+    c->mk.M = M;
+    size_t bytes;
+    {
+        Carver cv{nullptr};
+        cv.take<GelDev>(std::max(1, n_gels));
+        for (int i = 0; i < 5; i++) cv.take<float4>(std::max(1, M));
+        for (int i = 0; i < 3; i++) cv.take<float>(std::max(1, M));
+        cv.take<int>(std::max(1, M));
+        cv.take<int4>(std::max(1, M));
+        for (int i = 0; i < 3; i++) cv.take<float4>(std::max(1, M));
+        cv.take<float>(std::max(1, M));
+        cv.take<Box>(kMaxBoxes);
+        cv.take<Ctl>(1);
+        bytes = align_up(cv.off, 256);
+    }
+    cudaError_t e = cudaMalloc(&c->arena, bytes);
+    if (e != cudaSuccess) {
+        delete c;
+        return fail(GLSM_ERR_NOMEM, "coupler allocation: %s", cudaGetErrorString(e));
+    }
+    Carver cv{(char*)c->arena};
+    c->d_gels = cv.take<GelDev>(std::max(1, n_gels));
+    MarkerDev& mk = c->mk;
+    mk.lag = cv.take<float4>(std::max(1, M));
+    mk.Vl = cv.take<float4>(std::max(1, M));
+    mk.Ul = cv.take<float4>(std::max(1, M));
+    mk.Fdrag = cv.take<float4>(std::max(1, M));
+    mk.Frep = cv.take<float4>(std::max(1, M));
+    mk.Cl = cv.take<float>(std::max(1, M));
+    mk.Dl = cv.take<float>(std::max(1, M));
+    mk.Sl = cv.take<float>(std::max(1, M));
+    mk.owner = cv.take<int>(std::max(1, M));
+    mk.base = cv.take<int4>(std::max(1, M));
+    mk.phx = cv.take<float4>(std::max(1, M));
+    mk.phy = cv.take<float4>(std::max(1, M));
+    mk.phz = cv.take<float4>(std::max(1, M));
+    mk.wsum = cv.take<float>(std::max(1, M));
+    mk.boxes = cv.take<Box>(kMaxBoxes);
+    c->d_ctl = cv.take<Ctl>(1);
+    std::vector<int> owner(M);
+    int off = 0;
+    for (int i = 0; i < n_gels; i++) {
+        glsm_gel_s* g = gels[i];
+        cudaStreamSynchronize(g->own);
+        g->coupler = c;
+        g->index = i;
+        g->d.marker_off = off;
+        for (int l = 0; l < g->d.M; l++) owner[off + l] = i;
+        off += g->d.M;
+        c->gels.push_back(g);
+    }
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaHostAlloc((void**)&c->h_ctl, sizeof(Ctl), cudaHostAllocDefault);
+    if (e == cudaSuccess) e = cudaMemset(c->arena, 0, bytes);
+    if (e == cudaSuccess && M) e = cudaMemcpy(mk.owner, owner.data(), M * sizeof(int), cudaMemcpyHostToDevice);
+    for (int i = 0; i < n_gels && e == cudaSuccess; i++)
+        e = cudaMemcpy(c->d_gels + i, &c->gels[i]->d, sizeof(GelDev), cudaMemcpyHostToDevice);
+    for (int i = 0; i < n_gels && e == cudaSuccess; i++)
+        e = cudaMemcpy(c->gels[i]->d_self, &c->gels[i]->d, sizeof(GelDev), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        for (auto* g : c->gels) {
+            g->coupler = nullptr;
+            g->index = -1;
+        }
+        if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+        if (c->ev_join) cudaEventDestroy(c->ev_join);
+        if (c->side) cudaStreamDestroy(c->side);
+        if (c->stream) cudaStreamDestroy(c->stream);
+        if (c->h_ctl) cudaFreeHost(c->h_ctl);
+        cudaFree(c->arena);
+        delete c;
+        return fail(GLSM_ERR_CUDA, "coupler initialisation: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return GLSM_OK;
+}
+
+int glsm_coupler_destroy(glsm_coupler c) {
+    if (!c) return GLSM_OK;
+    if (c->fluid) return fail(GLSM_ERR_STATE, "destroy the fluid before its coupler");
+    cudaStreamSynchronize(c->stream);
+    for (auto* g : c->gels) {
+        g->coupler = nullptr;
+        g->index = -1;
+    }
+    cudaEventDestroy(c->ev_fork);
+    cudaEventDestroy(c->ev_join);
+    cudaStreamDestroy(c->side);
+    cudaStreamDestroy(c->stream);
+    cudaFreeHost(c->h_ctl);
+    cudaFree(c->arena);
+    delete c;
+    return GLSM_OK;
+}
+
+int glsm_coupler_markers(glsm_coupler c) { return c ? c->mk.M : 0; }
+void* glsm_coupler_stream(glsm_coupler c) { return c ? (void*)c->stream : nullptr; }
+
+static GelArgs coupler_gel_args(glsm_coupler c, int phases, int iter_arg) {
+    GelArgs a{};
+    a.gels = c->d_gels;
+    a.first_gel = 0;
+    a.Mk = c->mk;
+    a.ctl = c->d_ctl;
+    a.phases = phases;
+    a.iter_arg = iter_arg;
+    if (c->fluid) {
+        a.nx = c->fluid->F.nx;
+        a.ny = c->fluid->F.ny;
+        a.nz = c->fluid->F.nz;
+        a.h = c->fluid->F.h;
+    }
+    a.g2l = c->g2l;
+    return a;
+}
+
+int glsm_coupler_pack(glsm_coupler c) {
+    if (!c) return fail(GLSM_ERR_ARG, "null coupler");
+    if (!c->fluid) return fail(GLSM_ERR_STATE, "create the fluid before packing markers");
+    CK(launch_gel(coupler_gel_args(c, kPhGather, 0), (int)c->gels.size(), c->stream));
+    return GLSM_OK;
+}
+
+int glsm_coupler_scatter(glsm_coupler c) {
+    if (!c) return fail(GLSM_ERR_ARG, "null coupler");
+    CK(launch_scatter(c->d_gels, c->mk, c->stream));
+    return GLSM_OK;
+}
+
+int glsm_coupler_repulsion(glsm_coupler c) {
+    if (!c) return fail(GLSM_ERR_ARG, "null coupler");
+    RepulsionArgs r{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 0};
+    CK(launch_repulsion(r, c->stream));
+    return GLSM_OK;
+}
+
+int glsm_coupler_read(glsm_coupler c, int field, float* dst, size_t count) {
+    if (!c || !dst) return fail(GLSM_ERR_ARG, "null argument");
+    const size_t M = c->mk.M;
+    const float4* v4 = nullptr;
+    const float* v1 = nullptr;
+    switch (field) {
+        case GLSM_MK_LAG: v4 = c->mk.lag; break;
+        case GLSM_MK_UL: v4 = c->mk.Ul; break;
+        case GLSM_MK_VL: v4 = c->mk.Vl; break;
+        case GLSM_MK_FDRAG: v4 = c->mk.Fdrag; break;
+        case GLSM_MK_FREP: v4 = c->mk.Frep; break;
+        case GLSM_MK_CL: v1 = c->mk.Cl; break;
+        case GLSM_MK_DL: v1 = c->mk.Dl; break;
+        case GLSM_MK_SL: v1 = c->mk.Sl; break;
+        default: return fail(GLSM_ERR_ARG, "unknown marker field %d", field);
+    }
+    const size_t need = v4 ? 3 * M : M;
+    if (count < need) return fail(GLSM_ERR_ARG, "marker field needs %zu floats", need);
+    CK(cudaStreamSynchronize(c->stream));
+    if (v1) {
+        CK(cudaMemcpy(dst, v1, M * sizeof(float), cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<float4> tmp(M);
+        CK(cudaMemcpy(tmp.data(), v4, M * sizeof(float4), cudaMemcpyDeviceToHost));
+        for (size_t l = 0; l < M; l++) {
+            dst[3 * l] = tmp[l].x;
+            dst[3 * l + 1] = tmp[l].y;
+            dst[3 * l + 2] = tmp[l].z;
+        }
+    }
+    return GLSM_OK;
+}
+
+// ===========================================================================
+// Fluid
+// ===========================================================================
+// Fluid ctor unit conversions in float (src/fluid.cu:167-229)
+static void fluid_units(float tau, float h, float& g2l, float& l2g, int& nsub) {
+    const float dt = 1e-3f, niu = 1e-6f;
+    const float dx_fluid = 40e-6f * h;
+    const float dt_fluid = (tau - 0.5f) * dx_fluid * dx_fluid / (3 * niu);
+    nsub = std::max(1, (int)llround(dt / dt_fluid));
+    g2l = h * dt_fluid / dt;
+    l2g = 1.0f / g2l;
+}
+
+int glsm_fluid_desc_default(glsm_fluid_desc* d, int nx, int ny, int nz) {
+    if (!d) return fail(GLSM_ERR_ARG, "null desc");
+    std::memset(d, 0, sizeof(*d));
+    d->nx = nx;
+    d->ny = ny;
+    d->nz = nz;
+    d->tau = 0.8f;
+    d->h = 0.5f;
+    d->beta = 1.0f;
+    if (const char* s = getenv("IBM_BETA")) d->beta = (float)atof(s);
+    d->ramp_steps = 20000.0f;
+    if (const char* s = getenv("IBM_RAMP_STEPS")) d->ramp_steps = std::fmax(0.0f, (float)atof(s));
+    float g2l, l2g;
+    fluid_units(d->tau, d->h, g2l, l2g, d->nsub);
+    d->storage = GLSM_STORE_F32;
+    d->fp16_scale = 1048576.0f;  // 2^20
+    return GLSM_OK;
+}
+
+__global__ void u_rest_kernel(float4* u, long long N);
+
+static StepArgs step_args(glsm_fluid f, int k, int iter_arg) {
+    StepArgs a{};
+    a.F = f->F;
+    a.Mk = f->c->mk;
+    a.ctl = f->c->d_ctl;
+    a.tickets = f->d_sync;
+    a.ibm_done = f->d_sync + f->F.nsub;
+    a.n_boxes = (int)f->c->gels.size();
+    a.n_ibm = (f->c->mk.M + kMarkersPerTask - 1) / kMarkersPerTask;
+    a.iter_arg = iter_arg;
+    a.k = k;
+    a.last = (k == f->F.nsub - 1);
+    return a;
+}
+
+int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out) {
+    if (!d || !c || !out) return fail(GLSM_ERR_ARG, "null argument");
+    if (c->fluid) return fail(GLSM_ERR_STATE, "coupler already has a fluid");
+    if (d->nx < 4 || d->ny < 4 || d->nz < 4) return fail(GLSM_ERR_ARG, "lattice must be >= 4 cells per axis");
+    const long long N = (long long)d->nx * d->ny * d->nz;
+    if (N > (1LL << 31) / 2) return fail(GLSM_ERR_ARG, "lattice too large");
+    if (d->nsub < 1 || d->nsub > 4096) return fail(GLSM_ERR_ARG, "nsub must be in [1, 4096]");
+    if (d->storage < 0 || d->storage > 2) return fail(GLSM_ERR_ARG, "unknown storage %d", d->storage);
+    if (!(d->tau > 0.5f) || !(d->h > 0.f)) return fail(GLSM_ERR_ARG, "tau must exceed 0.5 and h be positive");
+    auto* f = new glsm_fluid_s;
+    f->desc = *d;
+    FluidDev& F = f->F;
+    F.nx = d->nx;
+    F.ny = d->ny;
+    F.nz = d->nz;
+    F.N = N;
+    F.S = (long long)align_up((size_t)N, 64);
+    F.storage = d->storage;
+    F.scale = (d->storage == GLSM_STORE_F16) ? (d->fp16_scale > 0 ? d->fp16_scale : 1048576.0f) : 1.0f;
+    F.inv_scale = 1.0f / F.scale;
+    F.tau = d->tau;
+    F.omega = 1.0f / d->tau;
+    F.fpref = 1.0f - 0.5f / d->tau;
+    for (int i = 0; i < 3; i++) {
+        F.Fc[i] = d->force[i];
+        F.per[i] = d->periodic[i] ? 1 : 0;
+    }
+    F.h = d->h;
+    F.dtc = 1e-3f;  // FluidParams dt (fluid.cu:167)
+    F.Dc = 1.0f;    // FluidParams D (fluid.cu:193)
+    F.inv_dx = 1.0f;  // FluidParams dx = dy = dz = 1 (fluid.cu:190-192)
+    F.beta = d->beta;
+    F.ramp_steps = d->ramp_steps;
+    F.nsub = d->nsub;
+    const size_t esz = (d->storage == GLSM_STORE_F32) ? 4 : 2;
+    size_t bytes;
+    {
+        Carver cv{nullptr};
+        cv.take<char>(19 * (size_t)F.S * esz);
+        cv.take<float4>(N);
+        cv.take<float4>(N);
+        for (int i = 0; i < 3; i++) cv.take<float>(N);
+        cv.take<unsigned>(2 * (size_t)d->nsub);
+        bytes = align_up(cv.off, 256);
+    }
+    cudaError_t e = cudaMalloc(&f->arena, bytes);
+    if (e != cudaSuccess) {
+        delete f;
+        return fail(GLSM_ERR_NOMEM, "lattice allocation of %zu bytes: %s", bytes, cudaGetErrorString(e));
+    }
+    f->bytes = bytes;
+    Carver cv{(char*)f->arena};
+    F.pop = cv.take<char>(19 * (size_t)F.S * esz);
+    F.u = cv.take<float4>(N);
+    F.Fibm = cv.take<float4>(N);
+    F.c[0] = cv.take<float>(N);
+    F.c[1] = cv.take<float>(N);
+    F.source = cv.take<float>(N);
+    f->d_sync = cv.take<unsigned>(2 * (size_t)d->nsub);
+    // rest state: zero deviations (f = w), u = 0, c = 0 (k_init, fluid_kernels.cu:84-96)
+    e = cudaMemsetAsync(f->arena, 0, bytes, c->stream);
+    if (e == cudaSuccess) {
+        u_rest_kernel<<<(unsigned)((N + 255) / 256), 256, 0, c->stream>>>(F.u, N);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        cudaFree(f->arena);
+        delete f;
+        return fail(GLSM_ERR_CUDA, "lattice initialisation: %s", cudaGetErrorString(e));
+    }
+    int nsub_phys;
+    fluid_units(d->tau, d->h, c->g2l, c->l2g, nsub_phys);
+    f->c = c;
+    c->fluid = f;
+    // the gels' gather now knows the lattice
+    *out = f;
+    return GLSM_OK;
+}
+
+int glsm_fluid_destroy(glsm_fluid f) {
+    if (!f) return GLSM_OK;
+    cudaStreamSynchronize(f->c->stream);
+    for (auto& row : f->graph)
+        for (auto& g : row)
+            if (g) cudaGraphExecDestroy(g);
+    if (f->scratch) cudaFree(f->scratch);
+    cudaFree(f->arena);
+    f->c->fluid = nullptr;
+    delete f;
+    return GLSM_OK;
+}
+
+int glsm_fluid_units(glsm_fluid f, float out[2]) {
+    if (!f || !out) return fail(GLSM_ERR_ARG, "null argument");
+    out[0] = f->c->g2l;
+    out[1] = f->c->l2g;
+    return GLSM_OK;
+}
+
+int glsm_fluid_info(glsm_fluid f, int64_t out[8]) {
+    if (!f || !out) return fail(GLSM_ERR_ARG, "null argument");
+    out[0] = f->F.nx;
+    out[1] = f->F.ny;
+    out[2] = f->F.nz;
+    out[3] = f->F.N;
+    out[4] = f->F.nsub;
+    out[5] = f->F.storage;
+    out[6] = (int64_t)f->bytes;
+    out[7] = f->substeps;
+    return GLSM_OK;
+}
+
+// the substeps of one gel step (Fluid::stepVelocity)
+static int enqueue_velocity(glsm_fluid f, int iter_arg, cudaStream_t s) {
+    const int nsub = f->F.nsub;
+    const int p0 = (int)(f->substeps & 1);
+    CK(cudaMemsetAsync(f->d_sync, 0, 2 * sizeof(unsigned) * nsub, s));
+    for (int k = 0; k < nsub; k++) CK(launch_substep(step_args(f, k, iter_arg), (p0 + k) & 1, s));
+    return GLSM_OK;
+}
+
+int glsm_fluid_step_velocity(glsm_fluid f, int iter) {
+    if (!f || iter < 0) return fail(GLSM_ERR_ARG, "bad argument");
+    int r = enqueue_velocity(f, iter, f->c->stream);
+    if (r) return r;
+    f->substeps += f->F.nsub;
+    return GLSM_OK;
+}
+
+int glsm_fluid_step_concentration(glsm_fluid f, int iter) {
+    if (!f || iter < 0) return fail(GLSM_ERR_ARG, "bad argument");
+    glsm_coupler c = f->c;
+    MarkerArgs m{c->d_gels, c->mk, f->F.c[f->cur], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 0};
+    CK(launch_conc_markers(m, c->stream));
+    ConcArgs a{f->F, c->mk, c->d_ctl, (int)c->gels.size(), f->cur, 0};
+    CK(launch_conv_diff(a, c->stream));
+    f->cur ^= 1;
+    return GLSM_OK;
+}
+
+__global__ void set_iter_kernel(Ctl* ctl, int iter) { ctl->iter = iter; }
+
+// one whole coupled iteration; iter_arg < 0 reads the iteration from the
+// control block (graph mode) and advances it at the end
+static int enqueue_iteration(glsm_fluid f, int iter_arg, int p0, int cur) {
+    glsm_coupler c = f->c;
+    cudaStream_t s = c->stream;
+    const int nsub = f->F.nsub;
+    CK(cudaMemsetAsync(f->d_sync, 0, 2 * sizeof(unsigned) * nsub, s));
+    const int phases = kPhElastic | kPhChem | kPhRecord | kPhGather | kPhAuto;
+    CK(launch_gel(coupler_gel_args(c, phases, iter_arg), (int)c->gels.size(), s));
+    // markers' concentration exchange and repulsion run beside the substeps
+    CK(cudaEventRecord(c->ev_fork, s));
+    CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
+    MarkerArgs m{c->d_gels, c->mk, f->F.c[cur], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 1};
+    CK(launch_conc_markers(m, c->side));
+    RepulsionArgs r{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 1};
+    CK(launch_repulsion(r, c->side));
+    CK(cudaEventRecord(c->ev_join, c->side));
+    for (int k = 0; k < nsub; k++) CK(launch_substep(step_args(f, k, iter_arg), (p0 + k) & 1, s));
+    CK(cudaStreamWaitEvent(s, c->ev_join, 0));
+    ConcArgs a{f->F, c->mk, c->d_ctl, (int)c->gels.size(), cur, iter_arg < 0 ? 1 : 0};
+    CK(launch_conv_diff(a, s));
+    return GLSM_OK;
+}
+
+static int get_graph(glsm_fluid f, int p0, int cur, cudaGraphExec_t* out) {
+    if (f->graph[p0][cur]) {
+        *out = f->graph[p0][cur];
+        return GLSM_OK;
+    }
+    cudaStream_t s = f->c->stream;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int r = enqueue_iteration(f, -1, p0, cur);
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (r) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail(GLSM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&f->graph[p0][cur], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(GLSM_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    *out = f->graph[p0][cur];
+    return GLSM_OK;
+}
+
+int glsm_fluid_run(glsm_fluid f, int iter0, int n) {
+    if (!f || iter0 < 0 || n < 0) return fail(GLSM_ERR_ARG, "bad argument");
+    if (n == 0) return GLSM_OK;
+    glsm_coupler c = f->c;
+    set_iter_kernel<<<1, 1, 0, c->stream>>>(c->d_ctl, iter0);
+    CK(cudaGetLastError());
+    static const bool eager = getenv("GLSM_EAGER") != nullptr;  // debugging: no graphs
+    for (int it = 0; it < n; it++) {
+        const int p0 = (int)(f->substeps & 1);
+        if (eager) {
+            int r = enqueue_iteration(f, iter0 + it, p0, f->cur);
+            if (r) return r;
+        } else {
+            cudaGraphExec_t ge;
+            int r = get_graph(f, p0, f->cur, &ge);
+            if (r) return r;
+            CK(cudaGraphLaunch(ge, c->stream));
+        }
+        f->substeps += f->F.nsub;
+        f->cur ^= 1;
+    }
+    if (eager) {
+        set_iter_kernel<<<1, 1, 0, c->stream>>>(c->d_ctl, iter0 + n);
+        CK(cudaGetLastError());
+    }
+    return GLSM_OK;
+}
+
+int glsm_fluid_sync(glsm_fluid f) {
+    if (!f) return fail(GLSM_ERR_ARG, "null fluid");
+    glsm_coupler c = f->c;
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaMemcpy(c->h_ctl, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+    if (c->h_ctl->error) {
+        const int err = c->h_ctl->error;
+        CK(cudaMemset(&c->d_ctl->error, 0, sizeof(int)));
+        return fail(GLSM_ERR_DEVICE, "device error flags 0x%x%s%s%s", err,
+                    (err & kErrIbmWait) ? " [IBM wait timed out]" : "",
+                    (err & kErrMarkerOut) ? " [marker stencil outside the lattice]" : "",
+                    (err & kErrNonFinite) ? " [non-finite gel state]" : "");
+    }
+    return GLSM_OK;
+}
+
+static int ensure_scratch(glsm_fluid f) {
+    if (!f->scratch) CK(cudaMalloc(&f->scratch, 19 * sizeof(float) * (size_t)f->F.N));
+    return GLSM_OK;
+}
+
+// u (to_float3 = 1) or rho (to_float3 = 0) out of the (ux, uy, uz, rho) cells
+__global__ void u_pack_kernel(const float4* u, long long N, float* out, int to_float3) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    const float4 v = u[i];
+    if (to_float3) {
+        out[3 * i] = v.x;
+        out[3 * i + 1] = v.y;
+        out[3 * i + 2] = v.z;
+    } else {
+        out[i] = v.w;
+    }
+}
+
+__global__ void u_rest_kernel(float4* u, long long N) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < N) u[i] = make_float4(0.f, 0.f, 0.f, 1.0f);
+}
+
+__global__ void u_unpack_kernel(const float* in, long long N, float4* u) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    u[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 1.0f);
+}
+
+int glsm_fluid_read(glsm_fluid f, int field, float* dst, size_t count) {
+    if (!f || !dst) return fail(GLSM_ERR_ARG, "null argument");
+    cudaStream_t s = f->c->stream;
+    const long long N = f->F.N;
+    const unsigned blocks = (unsigned)((N + 255) / 256);
+    int r;
+    switch (field) {
+        case GLSM_FLUID_POP: {
+            const size_t need = 19 * (size_t)N;
+            if (count < need) return fail(GLSM_ERR_ARG, "field needs %zu floats", need);
+            if ((r = ensure_scratch(f))) return r;
+            CK(launch_read_pop(f->F, (f->substeps & 1) == 0, f->scratch, s));
+            CK(cudaMemcpyAsync(dst, f->scratch, need * sizeof(float), cudaMemcpyDeviceToHost, s));
+            break;
+        }
+        case GLSM_FLUID_RHO: {
+            // d_rho of the reference: the density moment of the last substep's
+            // macros (k_macros), kept in u.w
+            if (count < (size_t)N) return fail(GLSM_ERR_ARG, "field needs %lld floats", N);
+            if ((r = ensure_scratch(f))) return r;
+            u_pack_kernel<<<blocks, 256, 0, s>>>(f->F.u, N, f->scratch, 0);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(dst, f->scratch, N * sizeof(float), cudaMemcpyDeviceToHost, s));
+            break;
+        }
+        case GLSM_FLUID_U: {
+            if (count < 3 * (size_t)N) return fail(GLSM_ERR_ARG, "field needs %lld floats", 3 * N);
+            if ((r = ensure_scratch(f))) return r;
+            u_pack_kernel<<<blocks, 256, 0, s>>>(f->F.u, N, f->scratch, 1);
+            CK(cudaGetLastError());
+            CK(cudaMemcpyAsync(dst, f->scratch, 3 * N * sizeof(float), cudaMemcpyDeviceToHost, s));
+            break;
+        }
+        case GLSM_FLUID_C1:
+            if (count < (size_t)N) return fail(GLSM_ERR_ARG, "field needs %lld floats", N);
+            CK(cudaMemcpyAsync(dst, f->F.c[f->cur], N * sizeof(float), cudaMemcpyDeviceToHost, s));
+            break;
+        default: return fail(GLSM_ERR_ARG, "unknown fluid field %d", field);
+    }
+    return glsm_fluid_sync(f);
+}
+
+int glsm_fluid_write(glsm_fluid f, int field, const float* src, size_t count) {
+    if (!f || !src) return fail(GLSM_ERR_ARG, "null argument");
+    cudaStream_t s = f->c->stream;
+    const long long N = f->F.N;
+    const unsigned blocks = (unsigned)((N + 255) / 256);
+    int r;
+    switch (field) {
+        case GLSM_FLUID_POP:
+            if (count != 19 * (size_t)N) return fail(GLSM_ERR_ARG, "populations hold %lld floats", 19 * N);
+            if ((r = ensure_scratch(f))) return r;
+            CK(cudaMemcpyAsync(f->scratch, src, count * sizeof(float), cudaMemcpyHostToDevice, s));
+            CK(launch_write_pop(f->F, f->scratch, s));
+            f->substeps &= ~1LL;  // natural layout from now on
+            break;
+        case GLSM_FLUID_U:
+            if (count != 3 * (size_t)N) return fail(GLSM_ERR_ARG, "u holds %lld floats", 3 * N);
+            if ((r = ensure_scratch(f))) return r;
+            CK(cudaMemcpyAsync(f->scratch, src, count * sizeof(float), cudaMemcpyHostToDevice, s));
+            u_unpack_kernel<<<blocks, 256, 0, s>>>(f->scratch, N, f->F.u);
+            CK(cudaGetLastError());
+            break;
+        case GLSM_FLUID_C1:
+            if (count != (size_t)N) return fail(GLSM_ERR_ARG, "c1 holds %lld floats", N);
+            CK(cudaMemcpyAsync(f->F.c[f->cur], src, N * sizeof(float), cudaMemcpyHostToDevice, s));
+            break;
+        default: return fail(GLSM_ERR_ARG, "field %d is not writable", field);
+    }
+    CK(cudaStreamSynchronize(s));
+    return GLSM_OK;
+}
+
+}  // extern "C"

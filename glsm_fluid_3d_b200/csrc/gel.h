@@ -1,0 +1,50 @@
+// gel.h -- launch arguments and launchers of the gel/marker kernels (gel.cu)
+#pragma once
+#include "glsm_internal.h"
+
+namespace glsm {
+
+// phases of the one-CTA-per-gel kernel
+enum : int {
+    kPhElastic = 1,   // Gel::stepElasticity: mechanics when iter % 5 == 0, then setZero
+    kPhChem = 2,      // Gel::stepChemistry
+    kPhGather = 4,    // Coupler::packFromGels for this gel + stencil cache + box
+    kPhRecord = 8,    // Gel::recordCenter (time series)
+    kPhAuto = 16,     // honour active_from: skip before it, fire the pulse at it
+};
+
+struct GelArgs {
+    GelDev* gels;      // device array
+    int first_gel;     // blockIdx.x + first_gel is the gel handled by a CTA
+    MarkerDev Mk;
+    Ctl* ctl;
+    int phases;
+    int iter_arg;      // >= 0: iteration number; < 0: read Ctl::iter
+    int nx, ny, nz;    // lattice (for the stencil cache)
+    float h;
+    float g2l;         // gel -> lattice velocity factor
+};
+
+struct MarkerArgs {
+    GelDev* gels;
+    MarkerDev Mk;
+    const float* c;    // current concentration
+    float* source;
+    int nx, ny, nz;
+    float h;
+    int scatter;       // also do un_robin -= Sl (Coupler::scatterToGels, C2 part)
+};
+
+struct RepulsionArgs {
+    GelDev* gels;
+    MarkerDev Mk;
+    float delta, gamma;
+    int scatter;       // also do Fn_robin -= Frep
+};
+
+cudaError_t launch_gel(const GelArgs& a, int n_gels, cudaStream_t s);
+cudaError_t launch_conc_markers(const MarkerArgs& a, cudaStream_t s);
+cudaError_t launch_repulsion(const RepulsionArgs& a, cudaStream_t s);
+cudaError_t launch_scatter(GelDev* gels, const MarkerDev& Mk, cudaStream_t s);
+
+}  // namespace glsm

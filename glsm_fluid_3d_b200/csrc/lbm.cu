@@ -1,0 +1,519 @@
+// lbm.cu -- the fluid side of one coupled iteration on sm_100a:
+//   * lbm_substep_kernel: one LBM substep = IBM (interpolate, penalty force,
+//     spread) + BGK/Guo collide + stream with half-way bounce-back, in place
+//     (AA pattern), populations stored as deviations from the rest weights.
+//   * conv_diff_kernel: upwind advection-diffusion of the concentration.
+//   * read_pop_kernel: populations back in the reference's natural layout.
+//
+// Reference semantics followed (lasite/gLSM_fluid_3D):
+//   Fluid::stepVelocity           src/fluid.cu:263-284 (substep order, IBM ramp)
+//   k_ibm_interpolate_velocity    src/fluid_kernels.cu:244-281
+//   k_scale_negbeta               src/fluid_kernels.cu:283-291
+//   k_ibm_spread_forces           src/fluid_kernels.cu:300-348
+//   k_macros / k_collide          src/fluid_kernels.cu:98-111, :125-142
+//   k_stream_bounce               src/fluid_kernels.cu:144-165
+//   k_convection_diffusion        src/fluid_kernels.cu:177-242
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "d3q19.cuh"
+#include "glsm_internal.h"
+#include "lbm.h"
+
+namespace glsm {
+
+// ---------------------------------------------------------------------------
+// population storage: FP32 deviations, or FP16 / BF16 deviations (scaled)
+// ---------------------------------------------------------------------------
+template <int ST>
+struct PopIO;
+template <>
+struct PopIO<kStoreF32> {
+    using T = float;
+    static __device__ __forceinline__ float ld(const T* p, float) { return *p; }
+    static __device__ __forceinline__ void st(T* p, float v, float) { *p = v; }
+};
+template <>
+struct PopIO<kStoreF16> {
+    using T = __half;
+    static __device__ __forceinline__ float ld(const T* p, float inv_scale) { return __half2float(*p) * inv_scale; }
+    static __device__ __forceinline__ void st(T* p, float v, float scale) { *p = __float2half_rn(v * scale); }
+};
+template <>
+struct PopIO<kStoreBF16> {
+    using T = __nv_bfloat16;
+    static __device__ __forceinline__ float ld(const T* p, float inv_scale) {
+        return __bfloat162float(*p) * inv_scale;
+    }
+    static __device__ __forceinline__ void st(T* p, float v, float scale) { *p = __float2bfloat16_rn(v * scale); }
+};
+
+__device__ __forceinline__ int current_iter(int iter_arg, const Ctl* ctl) {
+    return iter_arg >= 0 ? iter_arg : ctl->iter;
+}
+
+// IBM penalty ramp of Fluid::stepVelocity (src/fluid.cu:265-270), float arithmetic
+__device__ __forceinline__ float beta_eff(float beta, float ramp_steps, int iter) {
+    float ramp = (ramp_steps <= 0.0f) ? 1.0f : fminf(1.0f, (float)(iter + 1) / ramp_steps);
+    return beta * ramp;
+}
+
+__device__ __forceinline__ float comp4(const float4& v, int a) {
+    return a == 0 ? v.x : (a == 1 ? v.y : (a == 2 ? v.z : v.w));
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Tile extent (inclusive cell ranges per axis, conservative) of the linear cell
+// range [c0, c1].
+struct TileExt {
+    int x0, x1, y0, y1, z0, z1;
+};
+__device__ __forceinline__ TileExt tile_extent(long long c0, long long c1, int nx, int ny) {
+    const long long nxy = (long long)nx * ny;
+    TileExt e;
+    e.z0 = (int)(c0 / nxy);
+    e.z1 = (int)(c1 / nxy);
+    if (e.z0 != e.z1) {
+        e.y0 = 0;
+        e.y1 = ny - 1;
+        e.x0 = 0;
+        e.x1 = nx - 1;
+        return e;
+    }
+    long long r0 = c0 - (long long)e.z0 * nxy, r1 = c1 - (long long)e.z0 * nxy;
+    e.y0 = (int)(r0 / nx);
+    e.y1 = (int)(r1 / nx);
+    if (e.y0 != e.y1) {
+        e.x0 = 0;
+        e.x1 = nx - 1;
+    } else {
+        e.x0 = (int)(r0 - (long long)e.y0 * nx);
+        e.x1 = (int)(r1 - (long long)e.y0 * nx);
+    }
+    return e;
+}
+
+__device__ __forceinline__ bool overlaps(const Box& b, const TileExt& e) {
+    return b.x0 <= e.x1 && b.x1 >= e.x0 && b.y0 <= e.y1 && b.y1 >= e.y0 && b.z0 <= e.z1 && b.z1 >= e.z0;
+}
+__device__ __forceinline__ bool inside(const Box& b, int x, int y, int z) {
+    return x >= b.x0 && x <= b.x1 && y >= b.y0 && y <= b.y1 && z >= b.z0 && z <= b.z1;
+}
+
+// Collect into shared memory the marker boxes that overlap this CTA's tile.
+// Returns the count (all threads).  Uses one __syncthreads().
+__device__ __forceinline__ int tile_boxes(const Box* boxes, int n_boxes, const TileExt& e, Box* s_b, int* s_nb) {
+    if (threadIdx.x < n_boxes) {
+        Box b = boxes[threadIdx.x];
+        if (b.x0 <= b.x1 && overlaps(b, e)) {
+            int s = atomicAdd(s_nb, 1);
+            s_b[s] = b;
+        }
+    }
+    __syncthreads();
+    return *s_nb;
+}
+
+// ---------------------------------------------------------------------------
+// IBM task: one warp per marker.  Lane j owns stencil points j and j+32 of
+// the 4x4x4 stencil (point p = ax*16 + ay*4 + az, x outermost as in the
+// reference loops).  Interpolates u of the previous substep, forms the penalty
+// force beta_eff (Vl - Ul) and spreads it with vector float atomics.
+// ---------------------------------------------------------------------------
+__device__ void ibm_task(const StepArgs& a, unsigned task) {
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const FluidDev& F = a.F;
+    const MarkerDev& Mk = a.Mk;
+    const int l = (int)task * kMarkersPerTask + warp;
+    if (warp < kMarkersPerTask && l < Mk.M) {
+        const float be = beta_eff(F.beta, F.ramp_steps, current_iter(a.iter_arg, a.ctl));
+        const int4 b = Mk.base[l];
+        const float4 px = Mk.phx[l], py = Mk.phy[l], pz = Mk.phz[l];
+        const float ws = Mk.wsum[l];
+        const long long nx = F.nx, nxy = (long long)F.nx * F.ny;
+        float sx = 0.f, sy = 0.f, sz = 0.f;
+        long long cell[2];
+        float w[2];
+        bool ok[2];
+#pragma unroll
+        for (int j = 0; j < 2; j++) {
+            const int p = lane + 32 * j;
+            const int ax = p >> 4, ay = (p >> 2) & 3, az = p & 3;
+            ok[j] = ((b.w >> ax) & 1) && ((b.w >> (4 + ay)) & 1) && ((b.w >> (8 + az)) & 1);
+            w[j] = comp4(px, ax) * comp4(py, ay) * comp4(pz, az);
+            cell[j] = (long long)(b.x + ax) + (long long)(b.y + ay) * nx + (long long)(b.z + az) * nxy;
+            if (ok[j]) {
+                const float4 uu = F.u[cell[j]];
+                sx += uu.x * w[j];
+                sy += uu.y * w[j];
+                sz += uu.z * w[j];
+            }
+        }
+        sx = warp_sum(sx);
+        sy = warp_sum(sy);
+        sz = warp_sum(sz);
+        float4 Ul = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (ws > 0.0f) Ul = make_float4(sx / ws, sy / ws, sz / ws, 0.f);
+        const float4 Vl = Mk.Vl[l];
+        const float4 Fd = make_float4(be * (Vl.x - Ul.x), be * (Vl.y - Ul.y), be * (Vl.z - Ul.z), 0.f);
+        if (lane == 0) {
+            Mk.Ul[l] = Ul;
+            Mk.Fdrag[l] = Fd;
+        }
+        if (ws != 0.0f) {
+            const float inv_h3 = (float)(1.0 / (double)(F.h * F.h * F.h));
+            const float scale = inv_h3 / ws;
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                if (!ok[j]) continue;
+                const float wg = w[j] * scale;
+                atomicAdd(&F.Fibm[cell[j]], make_float4(Fd.x * wg, Fd.y * wg, Fd.z * wg, 0.f));
+            }
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(&a.ibm_done[a.k], 1u);
+    }
+}
+
+// bounded wait of a force-region tile for the IBM tasks of this substep
+__device__ __forceinline__ void wait_ibm(const StepArgs& a) {
+    if (threadIdx.x == 0) {
+        const volatile unsigned* flag = a.ibm_done + a.k;
+        const volatile int* err = &a.ctl->error;
+        unsigned spins = 0;
+        while (*flag < (unsigned)a.n_ibm) {
+            // give up after ~0.3 s (or at once when another tile already gave up)
+            if (++spins > (1u << 22) || (*err & kErrIbmWait)) {
+                atomicOr(&a.ctl->error, kErrIbmWait);
+                break;
+            }
+            __nanosleep(64);
+        }
+        __threadfence();
+    }
+    __syncthreads();
+}
+
+// ---------------------------------------------------------------------------
+// the substep kernel
+// ---------------------------------------------------------------------------
+template <int ST, int PARITY>
+__global__ void __launch_bounds__(kTile) lbm_substep_kernel(StepArgs a) {
+    using IO = PopIO<ST>;
+    using T = typename IO::T;
+    __shared__ unsigned s_ticket;
+    __shared__ int s_nb;
+    __shared__ Box s_b[kMaxBoxes];
+    if (threadIdx.x == 0) {
+        s_ticket = atomicAdd(&a.tickets[a.k], 1u);
+        s_nb = 0;
+    }
+    __syncthreads();
+    const unsigned t = s_ticket;
+    if (t < (unsigned)a.n_ibm) {
+        ibm_task(a, t);
+        return;
+    }
+    const FluidDev& F = a.F;
+    const int nx = F.nx, ny = F.ny, nz = F.nz;
+    const long long N = F.N, S = F.S, nxy = (long long)nx * ny;
+    const long long c0 = (long long)(t - a.n_ibm) * kTile;
+    if (c0 >= N) return;  // surplus CTA (never launched by the host; kept for safety)
+    const long long c1 = min(c0 + kTile - 1, N - 1);
+    const TileExt ext = tile_extent(c0, c1, nx, ny);
+    const int nb = tile_boxes(a.Mk.boxes, a.n_boxes, ext, s_b, &s_nb);
+    if (nb > 0) wait_ibm(a);
+
+    const long long i = c0 + threadIdx.x;
+    if (i > c1) return;
+    const int z = (int)(i / nxy);
+    const long long rem = i - (long long)z * nxy;
+    const int y = (int)(rem / nx);
+    const int x = (int)(rem - (long long)y * nx);
+
+    bool inb = false;
+    for (int j = 0; j < nb; j++) inb |= inside(s_b[j], x, y, z);
+
+    // neighbour offsets and wall flags per axis (m: minus side, p: plus side)
+    long long mo[3], po[3];
+    bool mw[3], pw[3];
+    {
+        const int c[3] = {x, y, z};
+        const int n[3] = {nx, ny, nz};
+        const long long st[3] = {1, nx, nxy};
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            mw[d] = false;
+            pw[d] = false;
+            if (c[d] > 0)
+                mo[d] = -st[d];
+            else if (F.per[d])
+                mo[d] = (long long)(n[d] - 1) * st[d];
+            else {
+                mo[d] = 0;
+                mw[d] = true;
+            }
+            if (c[d] < n[d] - 1)
+                po[d] = st[d];
+            else if (F.per[d])
+                po[d] = -(long long)(n[d] - 1) * st[d];
+            else {
+                po[d] = 0;
+                pw[d] = true;
+            }
+        }
+    }
+
+    T* P = reinterpret_cast<T*>(F.pop);
+    float d[19];
+    if (PARITY == 0) {
+#pragma unroll
+        for (int q = 0; q < 19; q++) d[q] = IO::ld(P + (long long)q * S + i, F.inv_scale);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            // arriving population f_q(x) = post-collision f_q(x - c_q), stored in
+            // slot opp(q) at x - c_q; across a wall it is the bounced opp(q)
+            // population of x itself, stored in slot q at x
+            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
+            const bool wall = (cx > 0 && mw[0]) || (cx < 0 && pw[0]) || (cy > 0 && mw[1]) || (cy < 0 && pw[1]) ||
+                              (cz > 0 && mw[2]) || (cz < 0 && pw[2]);
+            long long off = 0;
+            if (cx > 0) off += mo[0];
+            if (cx < 0) off += po[0];
+            if (cy > 0) off += mo[1];
+            if (cy < 0) off += po[1];
+            if (cz > 0) off += mo[2];
+            if (cz < 0) off += po[2];
+            const long long src = wall ? (long long)q * S + i : (long long)qopp(q) * S + i + off;
+            d[q] = IO::ld(P + src, F.inv_scale);
+        }
+    }
+
+    // body force: uniform F_const plus the IBM force inside the marker boxes
+    float Fx = F.Fc[0], Fy = F.Fc[1], Fz = F.Fc[2];
+    if (inb) {
+        const float4 fi = __ldcg(&F.Fibm[i]);
+        Fx += fi.x;
+        Fy += fi.y;
+        Fz += fi.z;
+        __stcg(&F.Fibm[i], make_float4(0.f, 0.f, 0.f, 0.f));
+    }
+
+    // moments (k_macros) and BGK + Guo forcing (k_collide) in deviation form
+    float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        drho += d[q];
+        if (qcx(q) > 0) jx += d[q];
+        if (qcx(q) < 0) jx -= d[q];
+        if (qcy(q) > 0) jy += d[q];
+        if (qcy(q) < 0) jy -= d[q];
+        if (qcz(q) > 0) jz += d[q];
+        if (qcz(q) < 0) jz -= d[q];
+    }
+    const float rho = 1.0f + drho;
+    const float ux = (jx + 0.5f * Fx) / rho, uy = (jy + 0.5f * Fy) / rho, uz = (jz + 0.5f * Fz) / rho;
+    const float uu = ux * ux + uy * uy + uz * uz;
+    const float uF = ux * Fx + uy * Fy + uz * Fz;
+    const float omega = F.omega, fp = F.fpref;
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        const float cx = (float)qcx(q), cy = (float)qcy(q), cz = (float)qcz(q);
+        const float cu = cx * ux + cy * uy + cz * uz;
+        const float cF = cx * Fx + cy * Fy + cz * Fz;
+        const float deq = qw(q) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - 1.5f * uu));
+        const float Ft = qw(q) * fp * (3.0f * cF + 9.0f * cu * cF - 3.0f * uF);
+        d[q] = d[q] - omega * (d[q] - deq) + Ft;
+    }
+
+    if (PARITY == 0) {
+#pragma unroll
+        for (int q = 0; q < 19; q++) IO::st(P + (long long)qopp(q) * S + i, d[q], F.scale);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            // post-collision f_q(x) streams to x + c_q (slot q), or bounces back
+            // into slot opp(q) of x when x + c_q lies beyond a wall
+            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
+            const bool wall = (cx > 0 && pw[0]) || (cx < 0 && mw[0]) || (cy > 0 && pw[1]) || (cy < 0 && mw[1]) ||
+                              (cz > 0 && pw[2]) || (cz < 0 && mw[2]);
+            long long off = 0;
+            if (cx > 0) off += po[0];
+            if (cx < 0) off += mo[0];
+            if (cy > 0) off += po[1];
+            if (cy < 0) off += mo[1];
+            if (cz > 0) off += po[2];
+            if (cz < 0) off += mo[2];
+            const long long dst = wall ? (long long)qopp(q) * S + i : (long long)q * S + i + off;
+            IO::st(P + dst, d[q], F.scale);
+        }
+    }
+    if (inb || a.last) F.u[i] = make_float4(ux, uy, uz, rho);
+}
+
+// ---------------------------------------------------------------------------
+// upwind advection + diffusion of the concentration (once per iteration)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kTile) conv_diff_kernel(ConcArgs a) {
+    __shared__ int s_nb;
+    __shared__ Box s_b[kMaxBoxes];
+    if (threadIdx.x == 0) {
+        s_nb = 0;
+        if (a.bump_iter && blockIdx.x == 0) a.ctl->iter += 1;  // nothing in this kernel reads it
+    }
+    __syncthreads();
+    const FluidDev& F = a.F;
+    const int nx = F.nx, ny = F.ny, nz = F.nz;
+    const long long N = F.N, nxy = (long long)nx * ny;
+    const long long c0 = (long long)blockIdx.x * kTile;
+    const long long c1 = min(c0 + kTile - 1, N - 1);
+    const TileExt ext = tile_extent(c0, c1, nx, ny);
+    const int nb = tile_boxes(a.Mk.boxes, a.n_boxes, ext, s_b, &s_nb);
+    const long long i = c0 + threadIdx.x;
+    if (i > c1) return;
+    const int z = (int)(i / nxy);
+    const long long rem = i - (long long)z * nxy;
+    const int y = (int)(rem / nx);
+    const int x = (int)(rem - (long long)y * nx);
+    bool inb = false;
+    for (int j = 0; j < nb; j++) inb |= inside(s_b[j], x, y, z);
+
+    const int xp = (x + 1 < nx) ? x + 1 : (F.per[0] ? 0 : x);
+    const int xm = (x - 1 >= 0) ? x - 1 : (F.per[0] ? nx - 1 : x);
+    const int yp = (y + 1 < ny) ? y + 1 : (F.per[1] ? 0 : y);
+    const int ym = (y - 1 >= 0) ? y - 1 : (F.per[1] ? ny - 1 : y);
+    const int zp = (z + 1 < nz) ? z + 1 : (F.per[2] ? 0 : z);
+    const int zm = (z - 1 >= 0) ? z - 1 : (F.per[2] ? nz - 1 : z);
+    const long long base = (long long)z * nxy + (long long)y * nx;
+    const long long ixp = base + xp, ixm = base + xm;
+    const long long iyp = (long long)z * nxy + (long long)yp * nx + x, iym = (long long)z * nxy + (long long)ym * nx + x;
+    const long long izp = (long long)zp * nxy + (long long)y * nx + x, izm = (long long)zm * nxy + (long long)y * nx + x;
+
+    const float* c1p = F.c[a.cur];
+    float* c2p = F.c[a.cur ^ 1];
+    const float* U = reinterpret_cast<const float*>(F.u);
+    const float c = c1p[i], cxp = c1p[ixp], cxm = c1p[ixm], cyp = c1p[iyp], cym = c1p[iym], czp = c1p[izp],
+                czm = c1p[izm];
+    const float ux = U[4 * i], uy = U[4 * i + 1], uz = U[4 * i + 2];
+    const float uL = 0.5f * (U[4 * ixm] + ux), uR = 0.5f * (ux + U[4 * ixp]);
+    const float vL = 0.5f * (U[4 * iym + 1] + uy), vR = 0.5f * (uy + U[4 * iyp + 1]);
+    const float wL = 0.5f * (U[4 * izm + 2] + uz), wR = 0.5f * (uz + U[4 * izp + 2]);
+    const float cLx = (uL >= 0.0f) ? cxm : c, cLy = (vL >= 0.0f) ? cym : c, cLz = (wL >= 0.0f) ? czm : c;
+    const float cRx = (uR >= 0.0f) ? c : cxp, cRy = (vR >= 0.0f) ? c : cyp, cRz = (wR >= 0.0f) ? c : czp;
+    const float ih = F.inv_dx, ih2 = ih * ih;
+    const float conv = -((uR * cRx - uL * cLx) * ih + (vR * cRy - vL * cLy) * ih + (wR * cRz - wL * cLz) * ih);
+    const float diff = F.Dc * ((cxm - 2.0f * c + cxp) * ih2 + (cym - 2.0f * c + cyp) * ih2 + (czm - 2.0f * c + czp) * ih2);
+    float src = 0.f;
+    if (inb) {
+        src = __ldcg(&F.source[i]);
+        __stcg(&F.source[i], 0.f);
+    }
+    c2p[i] = c + F.dtc * (conv + diff + src);
+}
+
+// ---------------------------------------------------------------------------
+// populations in the reference's layout f[i + q*N] (absolute values)
+// ---------------------------------------------------------------------------
+template <int ST>
+__global__ void read_pop_kernel(FluidDev F, int natural, float* out) {
+    using IO = PopIO<ST>;
+    using T = typename IO::T;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= F.N) return;
+    const int nx = F.nx, ny = F.ny, nz = F.nz;
+    const long long nxy = (long long)nx * ny, S = F.S;
+    const int z = (int)(i / nxy);
+    const long long rem = i - (long long)z * nxy;
+    const int y = (int)(rem / nx);
+    const int x = (int)(rem - (long long)y * nx);
+    const T* P = reinterpret_cast<const T*>(F.pop);
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        long long src = (long long)q * S + i;
+        if (!natural) {
+            const int sx = x - qcx(q), sy = y - qcy(q), sz = z - qcz(q);
+            int wx = F.per[0] ? (sx + nx) % nx : sx;
+            int wy = F.per[1] ? (sy + ny) % ny : sy;
+            int wz = F.per[2] ? (sz + nz) % nz : sz;
+            const bool in = wx >= 0 && wx < nx && wy >= 0 && wy < ny && wz >= 0 && wz < nz;
+            src = in ? (long long)qopp(q) * S + wx + (long long)wy * nx + (long long)wz * nxy : (long long)q * S + i;
+        }
+        out[(long long)q * F.N + i] = IO::ld(P + src, F.inv_scale) + qw(q);
+    }
+}
+
+// write absolute populations given in the reference layout; leaves the array
+// in natural layout (the caller resets its parity bookkeeping)
+template <int ST>
+__global__ void write_pop_kernel(FluidDev F, const float* in) {
+    using IO = PopIO<ST>;
+    using T = typename IO::T;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= F.N) return;
+    T* P = reinterpret_cast<T*>(F.pop);
+#pragma unroll
+    for (int q = 0; q < 19; q++) IO::st(P + (long long)q * F.S + i, in[(long long)q * F.N + i] - qw(q), F.scale);
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers
+// ---------------------------------------------------------------------------
+int lbm_grid(const StepArgs& a) {
+    return a.n_ibm + (int)((a.F.N + kTile - 1) / kTile);
+}
+
+cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
+    dim3 grid(lbm_grid(a)), block(kTile);
+#define GLSM_SUB(ST)                                                           \
+    if (parity)                                                                \
+        lbm_substep_kernel<ST, 1><<<grid, block, 0, s>>>(a);                   \
+    else                                                                       \
+        lbm_substep_kernel<ST, 0><<<grid, block, 0, s>>>(a);
+    switch (a.F.storage) {
+        case kStoreF32: GLSM_SUB(kStoreF32); break;
+        case kStoreF16: GLSM_SUB(kStoreF16); break;
+        case kStoreBF16: GLSM_SUB(kStoreBF16); break;
+        default: return cudaErrorInvalidValue;
+    }
+#undef GLSM_SUB
+    return cudaGetLastError();
+}
+
+cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s) {
+    dim3 grid((unsigned)((a.F.N + kTile - 1) / kTile)), block(kTile);
+    conv_diff_kernel<<<grid, block, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_read_pop(const FluidDev& F, int natural, float* out, cudaStream_t s) {
+    dim3 grid((unsigned)((F.N + 255) / 256)), block(256);
+    switch (F.storage) {
+        case kStoreF32: read_pop_kernel<kStoreF32><<<grid, block, 0, s>>>(F, natural, out); break;
+        case kStoreF16: read_pop_kernel<kStoreF16><<<grid, block, 0, s>>>(F, natural, out); break;
+        case kStoreBF16: read_pop_kernel<kStoreBF16><<<grid, block, 0, s>>>(F, natural, out); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_write_pop(const FluidDev& F, const float* in, cudaStream_t s) {
+    dim3 grid((unsigned)((F.N + 255) / 256)), block(256);
+    switch (F.storage) {
+        case kStoreF32: write_pop_kernel<kStoreF32><<<grid, block, 0, s>>>(F, in); break;
+        case kStoreF16: write_pop_kernel<kStoreF16><<<grid, block, 0, s>>>(F, in); break;
+        case kStoreBF16: write_pop_kernel<kStoreBF16><<<grid, block, 0, s>>>(F, in); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace glsm

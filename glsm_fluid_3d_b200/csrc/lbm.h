@@ -1,0 +1,35 @@
+// lbm.h -- launch arguments and launchers of the fluid kernels (lbm.cu)
+#pragma once
+#include "glsm_internal.h"
+
+namespace glsm {
+
+struct StepArgs {
+    FluidDev F;
+    MarkerDev Mk;
+    Ctl* ctl;
+    unsigned* tickets;   // [nsub] CTA tickets of this iteration's substeps
+    unsigned* ibm_done;  // [nsub] finished IBM task CTAs per substep
+    int n_boxes;
+    int n_ibm;           // IBM task CTAs at the head of each substep launch
+    int iter_arg;        // >= 0: iteration number; < 0: read Ctl::iter
+    int k;               // substep index within the iteration
+    int last;            // k == nsub - 1: write u for every cell
+};
+
+struct ConcArgs {
+    FluidDev F;
+    MarkerDev Mk;
+    Ctl* ctl;
+    int n_boxes;
+    int cur;        // index of the current concentration buffer
+    int bump_iter;  // advance Ctl::iter (graph mode)
+};
+
+int lbm_grid(const StepArgs& a);
+cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s);
+cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s);
+cudaError_t launch_read_pop(const FluidDev& F, int natural, float* out, cudaStream_t s);
+cudaError_t launch_write_pop(const FluidDev& F, const float* in, cudaStream_t s);
+
+}  // namespace glsm

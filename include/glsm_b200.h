@@ -1,0 +1,202 @@
+/*
+ * glsm_b200.h -- C ABI of libglsm_b200.so, the B200 (sm_100a) implementation of
+ * the coupled gel-fluid step of lasite/gLSM_fluid_3D.
+ *
+ * The three opaque handle types stand for the reference's three classes
+ * (src/gel.h:33-165 Gel, src/coupling.h:14-58 Coupler, src/fluid.h:24-84 Fluid).
+ * Each entry point names the reference member it replaces.  Conventions:
+ *   - every function returns an int status: GLSM_OK (0) or a negative code;
+ *     glsm_last_error() gives a one-line message (thread-local);
+ *   - host buffers are owned by the caller, device memory by the library;
+ *   - objects are created in the reference's order Gel -> Coupler -> Fluid
+ *     (src/fluid.cu:221-229 writes the unit conversions into the coupler and
+ *     every gel, so the fluid comes last);
+ *   - once coupled, all work of a system runs in program order on one CUDA
+ *     stream owned by the coupler (glsm_coupler_stream).
+ * Field layouts follow the reference: lattice cell index x + y*nx + z*nx*ny,
+ * populations f[i + q*N] in the D3Q19 order of src/fluid.cu:202-215, gel node
+ * vectors as xyz triples over (LX+2)(LY+2)(LZ+2) slots, element scalars over
+ * (LX+1)(LY+1)(LZ+1) slots (src/gel.cu:116-119).
+ */
+#ifndef GLSM_B200_H
+#define GLSM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GLSM_OK 0
+#define GLSM_ERR_ARG (-1)    /* invalid argument or size */
+#define GLSM_ERR_CUDA (-2)   /* a CUDA runtime call failed */
+#define GLSM_ERR_STATE (-3)  /* call not valid in the object's current state */
+#define GLSM_ERR_DEVICE (-4) /* a kernel raised an error flag (see message) */
+#define GLSM_ERR_NOMEM (-5)  /* device allocation failed */
+
+/* population storage of the lattice */
+#define GLSM_STORE_F32 0  /* FP32 deviations f_q - w_q */
+#define GLSM_STORE_F16 1  /* FP16 deviations, scaled by fp16_scale */
+#define GLSM_STORE_BF16 2 /* BF16 deviations */
+
+typedef struct glsm_gel_s* glsm_gel;
+typedef struct glsm_coupler_s* glsm_coupler;
+typedef struct glsm_fluid_s* glsm_fluid;
+
+/* gel fields (FP64, reference layout) for glsm_gel_read / _write / _device_ptr */
+enum glsm_gel_field {
+    GLSM_GEL_RN = 0,       /* m_drn      node positions (3 per node slot)     */
+    GLSM_GEL_VELN = 1,     /* m_dVeln    node (polymer) velocities            */
+    GLSM_GEL_VELS = 2,     /* m_dVels    solvent velocities                   */
+    GLSM_GEL_FN = 3,       /* m_dFn      nodal forces                         */
+    GLSM_GEL_UM = 4,       /* m_dum      activator per element slot           */
+    GLSM_GEL_VM = 5,       /* m_dvm      catalyst per element slot            */
+    GLSM_GEL_WM = 6,       /* m_dwm      polymer volume fraction              */
+    GLSM_GEL_UN_NORM = 7,  /* m_dun_norm nodal normalised activator           */
+    GLSM_GEL_VN_NORM = 8,  /* m_dvn_norm                                      */
+    GLSM_GEL_T0 = 9,       /* m_dT0m                                          */
+    GLSM_GEL_T1 = 10,      /* m_dT1m                                          */
+    GLSM_GEL_T2 = 11,      /* m_dT2m                                          */
+    GLSM_GEL_RM = 12,      /* m_drm      element centres (3 per element slot) */
+    GLSM_GEL_NMSM = 13,    /* m_dnmSm    face area vectors (18 per element)   */
+    GLSM_GEL_VOLM = 14,    /* m_dVolm                                         */
+    GLSM_GEL_PREM = 15,    /* m_dPrem                                         */
+    GLSM_GEL_UN_ROBIN = 16,/* m_dun_robin                                     */
+    GLSM_GEL_UM_NORM = 17, /* m_dum_norm                                      */
+    GLSM_GEL_VM_NORM = 18, /* m_dvm_norm                                      */
+    GLSM_GEL_WMP = 19,     /* m_dwmp                                          */
+    GLSM_GEL_FN_ROBIN = 20,/* m_dFn_robin                                     */
+    GLSM_GEL_RM_LOC = 21,  /* m_drm_loc  (24 per element)                     */
+    GLSM_GEL_NFIELDS = 22
+};
+
+/* lattice fields for glsm_fluid_read / _write (FP32, reference layout) */
+enum glsm_fluid_field {
+    GLSM_FLUID_POP = 0, /* d_f after the last substep: 19*N absolute populations */
+    GLSM_FLUID_RHO = 1, /* d_rho: N (computed from the populations)              */
+    GLSM_FLUID_U = 2,   /* d_u: 3*N, velocity of the last substep's macros       */
+    GLSM_FLUID_C1 = 3   /* d_c1: N, concentration                                */
+};
+
+/* marker fields of a coupler for glsm_coupler_read (FP32) */
+enum glsm_marker_field {
+    GLSM_MK_LAG = 0,   /* d_lag_all_   3*M */
+    GLSM_MK_UL = 1,    /* d_Ul_all_    3*M */
+    GLSM_MK_VL = 2,    /* d_Vl_all_    3*M */
+    GLSM_MK_FDRAG = 3, /* d_Fdrag_all_ 3*M */
+    GLSM_MK_FREP = 4,  /* d_Frep_all_  3*M */
+    GLSM_MK_CL = 5,    /* d_Cl_all_    M   */
+    GLSM_MK_DL = 6,    /* d_Dl_all_    M   */
+    GLSM_MK_SL = 7     /* d_Sl_all_    M   */
+};
+
+/* lattice description; glsm_fluid_desc_default fills the reference's values */
+typedef struct glsm_fluid_desc {
+    int nx, ny, nz;      /* lattice cells per axis (any size >= 4)                   */
+    int nsub;            /* LBM substeps per gel step (reference: 25, fluid.cu:194-197) */
+    int storage;         /* GLSM_STORE_*                                             */
+    float tau;           /* BGK relaxation time (0.8, fluid.cu:184)                  */
+    float beta;          /* IBM penalty (1.0 or $IBM_BETA, fluid.cu:198-201)          */
+    float ramp_steps;    /* IBM ramp length (20000 or $IBM_RAMP_STEPS, fluid.cu:265)  */
+    float force[3];      /* uniform body force F_const (0, fluid.cu:219)              */
+    int periodic[3];     /* periodic axes (the reference walls all six faces)         */
+    float fp16_scale;    /* power-of-two scale of FP16 deviations (default 2^20)       */
+    float h;             /* physical length of a lattice cell (0.5, fluid.cu:168)     */
+} glsm_fluid_desc;
+
+const char* glsm_last_error(void);
+int glsm_version(void);
+
+/* ---- Gel ---------------------------------------------------------------- */
+/* Gel::Gel(int3 gelSize, double3 gelPosition, int gelType, int gel_id, int time)
+ * src/gel.h:35, src/gel.cu:555-663 (time = 0; steady state by bisection,
+ * gel.cu:424-450; node lattice, gel.cu:179-219; surface order, gel.cu:161-177) */
+int glsm_gel_create(int sx, int sy, int sz, double px, double py, double pz, int gel_type, int gel_id,
+                    glsm_gel* out);
+/* Gel::~Gel, src/gel.cu:665-668 */
+int glsm_gel_destroy(glsm_gel g);
+/* sizes: LX, LY, LZ, element slots, node slots, markers, gel id, gel type */
+int glsm_gel_info(glsm_gel g, int64_t out[8]);
+/* GelParams uss, vss, wss (src/gel.h:12) */
+int glsm_gel_steady_state(glsm_gel g, double out[3]);
+/* Gel::stepElasticity(int iter), src/gel.cu:682-698 */
+int glsm_gel_step_elasticity(glsm_gel g, int iter);
+/* Gel::stepChemistry(int iter), src/gel.cu:700-704 */
+int glsm_gel_step_chemistry(glsm_gel g, int iter);
+/* Gel::recordCenter(int iter), src/gel.cu:706-713: one record every `every`
+ * iterations into a ring of `capacity` records (set by glsm_gel_series_config) */
+int glsm_gel_record_center(glsm_gel g, int iter);
+/* records of 12 doubles: iter, rn(3), Fn(3), Veln(3) of the centre node, vm, wm
+ * of the centre element (the columns of gel<id>bodycenter.dat, gel.cu:505-537) */
+int glsm_gel_series_config(glsm_gel g, int every, int capacity);
+int glsm_gel_series_read(glsm_gel g, double* dst, size_t count);
+/* Gel::resetToQuiescent(), src/gel.cu:731-747 */
+int glsm_gel_reset_quiescent(glsm_gel g);
+/* Gel::fireExcitationPulse(), src/gel.cu:751-783 */
+int glsm_gel_fire_pulse(glsm_gel g);
+/* Gel::setAnchorZ(double), src/gel.cu:788-795 */
+int glsm_gel_set_anchor_z(glsm_gel g, double anchor_z);
+/* Gel::buildTubeMask(int, bool), src/gel.cu:811-867 */
+int glsm_gel_build_tube_mask(glsm_gel g, int wall_thickness, int circular);
+/* the drivers' delayed start (src/sim_array.cpp:86-103) for glsm_fluid_run:
+ * the gel is skipped before `iter` and fires its pulse at `iter` (0: always on) */
+int glsm_gel_set_active_from(glsm_gel g, int iter);
+/* seeded uniform noise in [-amplitude, amplitude) added to um and vm of the
+ * interior elements (splitmix64 keyed by seed, gel id, slot, field) */
+int glsm_gel_add_noise(glsm_gel g, uint64_t seed, double amplitude);
+/* host copies of a field (count = number of doubles); the write replaces the
+ * field (restart, src/gel.cu:221-282) */
+int glsm_gel_read(glsm_gel g, int field, double* dst, size_t count);
+int glsm_gel_write(glsm_gel g, int field, const double* src, size_t count);
+size_t glsm_gel_field_size(glsm_gel g, int field);
+/* device pointer of a field: the reference's public m_d* members */
+void* glsm_gel_device_ptr(glsm_gel g, int field);
+
+/* ---- Coupler ------------------------------------------------------------ */
+/* Coupler::Coupler(std::vector<Gel*>&), src/coupling.h:16, src/coupling.cu:50-80 */
+int glsm_coupler_create(const glsm_gel* gels, int n_gels, glsm_coupler* out);
+/* Coupler::~Coupler, src/coupling.cu:158-161 (gels stay alive) */
+int glsm_coupler_destroy(glsm_coupler c);
+/* Coupler::packFromGels(), src/coupling.cu:82-98 */
+int glsm_coupler_pack(glsm_coupler c);
+/* Coupler::scatterToGels(), src/coupling.cu:100-118 */
+int glsm_coupler_scatter(glsm_coupler c);
+/* Coupler::applyGelRepulsion(), src/coupling.cu:120-123 */
+int glsm_coupler_repulsion(glsm_coupler c);
+/* marker count M (sumGelBoundaryCount, src/coupling.h:47) */
+int glsm_coupler_markers(glsm_coupler c);
+int glsm_coupler_read(glsm_coupler c, int field, float* dst, size_t count);
+/* the system stream (a cudaStream_t) */
+void* glsm_coupler_stream(glsm_coupler c);
+
+/* ---- Fluid -------------------------------------------------------------- */
+int glsm_fluid_desc_default(glsm_fluid_desc* d, int nx, int ny, int nz);
+/* Fluid::Fluid(int3 fluidSize, int time, Coupler*), src/fluid.h:26,
+ * src/fluid.cu:152-232; lattice dims and nsub are given directly */
+int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out);
+/* Fluid::~Fluid, src/fluid.cu:234-237 */
+int glsm_fluid_destroy(glsm_fluid f);
+/* Fluid::stepVelocity(int iter), src/fluid.cu:263-284 */
+int glsm_fluid_step_velocity(glsm_fluid f, int iter);
+/* Fluid::stepConcentration(int iter), src/fluid.cu:251-261 */
+int glsm_fluid_step_concentration(glsm_fluid f, int iter);
+/* n whole coupled iterations iter0 .. iter0+n-1 in the order of src/sim.cpp:97-112
+ * (gels, pack, stepVelocity, stepConcentration, repulsion, scatter), each one a
+ * CUDA graph launch; asynchronous on the system stream */
+int glsm_fluid_run(glsm_fluid f, int iter0, int n);
+/* wait for the system stream and report device-side error flags */
+int glsm_fluid_sync(glsm_fluid f);
+/* host copies of lattice fields (FP32, reference layout) */
+int glsm_fluid_read(glsm_fluid f, int field, float* dst, size_t count);
+/* replace populations (GLSM_FLUID_POP, absolute values), u (GLSM_FLUID_U) or c1 */
+int glsm_fluid_write(glsm_fluid f, int field, const float* src, size_t count);
+/* nx, ny, nz, N, nsub, storage, device bytes, substeps done */
+int glsm_fluid_info(glsm_fluid f, int64_t out[8]);
+/* gel_to_lbm_vel and lbm_to_gel_vel (src/fluid.cu:221-222) */
+int glsm_fluid_units(glsm_fluid f, float out[2]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GLSM_B200_H */
