@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Coupled MLUPS of the gel-fluid step on B200.
+
+Workload (the reference's default configuration): a 101x101x101 D3Q19 lattice,
+two 6x6x6-element gels at (16.67, 25, 25) and (33.33, 25, 25) in physical units
+(the relative layout of src/sim.cpp:26-30), Nsub = 25 LBM substeps per gel
+step, seeded chemistry noise.  One "step" is one coupled iteration (gels, marker
+pack, 25 IBM+LBM substeps, concentration, repulsion, scatter).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|f16|bf16]
+    python bench.py --impl reference      # the reference's own CUDA kernels
+
+Prints one JSON line.  Multi-GPU runs are independent replicas (one per rank,
+launched by torch.distributed.run); the job time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+DIMS = (101, 101, 101)
+NSUB = 25
+GELS = [((6, 6, 6), (16.67, 25.0, 25.0)), ((6, 6, 6), (33.33, 25.0, 25.0))]
+SEED, AMP = 12345, 1e-3
+BYTES_PER_CELL = {"f32": 152, "f16": 76, "bf16": 76}  # one read + one write of 19 populations
+FLUSH_BYTES = 256 << 20  # > the 126 MB L2
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
+    return p.parse_args()
+
+
+def workload_desc(storage):
+    return {
+        "workload": "101^3 D3Q19 lattice, two 6x6x6-element gels as in sim.cpp, Nsub=25, coupled step "
+                    "(gel mechanics+BZ chemistry, IBM, LBM, concentration)",
+        "lattice": list(DIMS), "gels": len(GELS), "gel_elements": [6, 6, 6], "nsub": NSUB,
+        "storage": storage, "parallelism": "replicas (one independent system per GPU)",
+        "l2": "256 MiB buffer written between timed steps",
+    }
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(storage):
+    """DRAM bytes per substep launch from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", f"lbm_substep_{storage}_101.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(self.index), "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        if not sm:
+            return None
+        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def make_system(storage):
+    from glsm_fluid_3d_b200 import System
+
+    s = System(*DIMS, nsub=NSUB, storage=storage)
+    for k, (size, pos) in enumerate(GELS):
+        s.add_gel(size, pos, 1, k + 1)
+        s.gel_noise(k, SEED, AMP)
+    s.finalize()
+    return s
+
+
+def cpu_baseline(budget_s):
+    """The FP64 oracle (OpenMP over all host cores) on a bounded sample of the workload."""
+    from oracle import pyoracle
+
+    cores = pyoracle.threads(os.cpu_count() or 1)
+    o = pyoracle.Oracle(*DIMS, nsub=NSUB)
+    for k, (size, pos) in enumerate(GELS):
+        o.add_gel(size, pos, 1, k + 1)
+        o.gel_noise(k, SEED, AMP)
+    o.finalize()
+    o.run(0, 1)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while n < 20:
+        o.run(1 + n, 1)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    cells = DIMS[0] * DIMS[1] * DIMS[2]
+    return {"value": round(cells * NSUB * n / dt / 1e6, 3), "unit": "MLUPS", "cores": cores, "kind": "port",
+            "sample": f"{n} coupled iterations of the same 101^3 two-gel workload after 1 warm-up, FP64 oracle "
+                      f"(oracle/glsm_oracle.cpp, OpenMP), {dt:.1f} s"}
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    s = make_system(args.storage)
+    fluid = s.fluid
+    stream = torch.cuda.ExternalStream(s.coupler.stream())
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    it = 0
+    for _ in range(args.warmup):
+        fluid.run(it, 1)
+        it += 1
+    fluid.sync()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    clocks = Clocks(local)
+    barrier()
+    clocks.start()
+    for k in range(K):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[k][0].record(stream)
+            fluid.run(it, 1)
+            ev[k][1].record(stream)
+        it += 1
+    stream.synchronize()
+    barrier()
+    clk = clocks.stop()
+    fluid.sync()
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    if world > 1:
+        t = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        t_ms = float(t.item())
+    N = DIMS[0] * DIMS[1] * DIMS[2]
+    value = world * N * NSUB * K / (t_ms / 1e3) / 1e6
+
+    # dominant kernel: the substep kernel, timed per launch on the system stream
+    prof = []
+    for _ in range(3):
+        prof.extend(fluid.profile_velocity(it).tolist())
+        s.coupler.packFromGels()  # keep the state consistent for what follows
+        fluid.stepConcentration(it)
+        it += 1
+    fluid.sync()
+    avg_ms = statistics.mean(prof)
+    bpc = BYTES_PER_CELL[args.storage]
+    achieved = bpc * N / (avg_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic = ncu_traffic(args.storage)
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+            "kernel": "lbm_substep_kernel", "bytes_per_launch": bpc * N, "avg_launch_ms": round(avg_ms, 5),
+            "note": "algorithmic bytes = one read + one write of 19 populations per cell; the 78 MB population "
+                    "array of 101^3 fits in L2, so achieved can exceed the HBM copy peak"}
+
+    # end to end through the C ABI with host buffers: restart the state from
+    # pinned host memory, run K iterations reading the gels' node velocities back
+    # every step (the reference driver's observable), read u and c back at the end
+    e2e = None
+    if not args.no_e2e:
+        pin = lambda n, dt: torch.empty(n, dtype=dt, pin_memory=True).numpy()  # noqa: E731
+        gels = s.gels
+        host_rn = [pin(g.nN * 3, torch.float64) for g in gels]
+        host_um = [pin(g.nE, torch.float64) for g in gels]
+        host_vm = [pin(g.nE, torch.float64) for g in gels]
+        host_vel = [pin(g.nN * 3, torch.float64) for g in gels]
+        host_u = pin(3 * N, torch.float32)
+        host_c = pin(N, torch.float32)
+        for g, a, b, c in zip(gels, host_rn, host_um, host_vm):
+            a[:] = g.read("rn")
+            b[:] = g.read("um")
+            c[:] = g.read("vm")
+        fluid.read_into("u", host_u)
+        fluid.read_into("c1", host_c)
+        h2d = sum(a.nbytes + b.nbytes + c.nbytes for a, b, c in zip(host_rn, host_um, host_vm)) + host_u.nbytes + \
+            host_c.nbytes
+        d2h = K * sum(v.nbytes for v in host_vel) + host_u.nbytes + host_c.nbytes
+        barrier()
+        t0 = time.perf_counter()
+        for g, a, b, c in zip(gels, host_rn, host_um, host_vm):
+            g.write("rn", a)
+            g.write("um", b)
+            g.write("vm", c)
+        fluid.write("u", host_u)
+        fluid.write("c1", host_c)
+        for k in range(K):
+            fluid.run(it, 1)
+            it += 1
+            for g, v in zip(gels, host_vel):
+                g.read_into("Veln", v)
+        fluid.read_into("u", host_u)
+        fluid.read_into("c1", host_c)
+        barrier()
+        t_e2e = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            t_e2e = float(t.item())
+        e2e = {"value": round(world * N * NSUB * K / t_e2e / 1e6, 1), "unit": "MLUPS",
+               "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": int(d2h / K),
+               "timing": "host wall clock around the whole job, device synchronised at both ends",
+               "job": "restart of gel chemistry/positions and u, c from pinned host memory (H2D), K fused "
+                      "iterations via glsm_fluid_run with every gel's Veln read back each step (D2H), final u "
+                      "and c read back (D2H); bytes are totals divided by K"}
+        assert np.isfinite(host_u).all()
+
+    base = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        base = cpu_baseline(args.cpu_seconds)
+
+    launches_per_step = 1 + 1 + 1 + 1 + NSUB + 1  # set-iter, gel, concentration markers, repulsion, substeps, conv-diff
+    line = {
+        "metric": "coupled MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": K,
+        "warmup": args.warmup, "ms_per_step": round(t_ms / K, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": args.storage, "data": "synthetic (seeded gel chemistry noise, fluid at rest)",
+        "config": workload_desc(args.storage), "roofline": roof, "cpu_baseline": base, "e2e": e2e,
+        "clocks": clk, "gpu_launches": launches_per_step * K,
+    }
+    s.close()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def run_reference(args, world, rank, local):
+    """The reference's own CUDA kernels (src/*.cu built unmodified for sm_100a)."""
+    if rank != 0:
+        return
+    import torch
+
+    from oracle import pyref
+
+    if not pyref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libglsm_ref.so was not built "
+                                                                "(the reference sources were absent at build time)"}))
+        return
+    torch.cuda.set_device(local)
+    r = pyref.Reference(*DIMS, nsub=NSUB)
+    for k, (size, pos) in enumerate(GELS):
+        r.add_gel(size, pos, 1, k + 1)
+        r.gel_noise(k, SEED, AMP)
+    r.set_params(beta=1.0, ramp_steps=20000.0)
+    r.finalize()
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    it = 0
+    r.time(it, args.warmup)
+    it += args.warmup
+    K = args.steps
+    clocks = Clocks(local)
+    torch.cuda.synchronize()
+    clocks.start()
+    t_ms = 0.0
+    for _ in range(K):
+        flush.zero_()  # legacy default stream: ordered with the reference's streams
+        t_ms += r.time(it, 1)
+        it += 1
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    r.close()
+    N = DIMS[0] * DIMS[1] * DIMS[2]
+    value = N * NSUB * K / (t_ms / 1e3) / 1e6
+    line = {
+        "impl": "reference", "metric": "coupled MLUPS", "value": round(value, 1), "unit": "MLUPS",
+        "n_gpus": world, "n_gpus_used": 1, "steps": K, "warmup": args.warmup, "ms_per_step": round(t_ms / K, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded gel chemistry noise, fluid at rest)", "config": workload_desc("f32"),
+        "cpu_baseline": {"value": round(value, 1), "unit": "MLUPS", "cores": None, "kind": "reference",
+                         "device": "cuda:0",
+                         "sample": f"{K} coupled iterations of the reference's CUDA kernels (its only "
+                                   f"implementation; oracle/_ref) in the stock call order of src/sim.cpp"},
+        "e2e": {"value": round(value, 1), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank, local)
+    else:
+        run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

@@ -127,6 +127,11 @@ class Gel:
         check(self.L.glsm_gel_read(self.h, fid, _dptr(buf), n), f"read {field}")
         return buf
 
+    def read_into(self, field, buf):
+        """Read a field into a caller-owned float64 array (e.g. pinned host memory)."""
+        fid = GEL_FIELDS[field] if isinstance(field, str) else int(field)
+        check(self.L.glsm_gel_read(self.h, fid, _dptr(buf), buf.size), f"read {field}")
+
     def write(self, field, values):
         fid = GEL_FIELDS[field] if isinstance(field, str) else int(field)
         v = np.ascontiguousarray(values, dtype=np.float64).ravel()
@@ -234,6 +239,12 @@ class Fluid:
 
     def sync(self):
         check(self.L.glsm_fluid_sync(self.h), "sync")
+
+    def profile_velocity(self, it):
+        """stepVelocity(it) with per-substep CUDA-event timings (ms) on the system stream."""
+        ms = np.zeros(self.Nsub, dtype=np.float32)
+        check(self.L.glsm_fluid_profile_velocity(self.h, int(it), _fptr(ms)), "profile_velocity")
+        return ms
 
     def units(self):
         out = (ctypes.c_float * 2)()

@@ -69,6 +69,7 @@ def lib():
         "glsm_fluid_write": [vp, i, P(f), ctypes.c_size_t],
         "glsm_fluid_info": [vp, P(ctypes.c_int64)],
         "glsm_fluid_units": [vp, P(f)],
+        "glsm_fluid_profile_velocity": [vp, i, P(f)],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

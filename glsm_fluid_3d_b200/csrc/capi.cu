@@ -758,6 +758,8 @@ static StepArgs step_args(glsm_fluid f, int k, int iter_arg) {
     a.iter_arg = iter_arg;
     a.k = k;
     a.last = (k == f->F.nsub - 1);
+    a.div_nx = make_fastdiv((unsigned)f->F.nx);
+    a.div_nxy = make_fastdiv((unsigned)(f->F.nx * f->F.ny));
     return a;
 }
 
@@ -766,7 +768,8 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     if (c->fluid) return fail(GLSM_ERR_STATE, "coupler already has a fluid");
     if (d->nx < 4 || d->ny < 4 || d->nz < 4) return fail(GLSM_ERR_ARG, "lattice must be >= 4 cells per axis");
     const long long N = (long long)d->nx * d->ny * d->nz;
-    if (N > (1LL << 31) / 2) return fail(GLSM_ERR_ARG, "lattice too large");
+    // 32-bit cell indices: 19 planes of padded length must stay below 2^32
+    if (N > 200000000LL) return fail(GLSM_ERR_ARG, "lattice too large (at most 2e8 cells)");
     if (d->nsub < 1 || d->nsub > 4096) return fail(GLSM_ERR_ARG, "nsub must be in [1, 4096]");
     if (d->storage < 0 || d->storage > 2) return fail(GLSM_ERR_ARG, "unknown storage %d", d->storage);
     if (!(d->tau > 0.5f) || !(d->h > 0.f)) return fail(GLSM_ERR_ARG, "tau must exceed 0.5 and h be positive");
@@ -896,7 +899,8 @@ int glsm_fluid_step_concentration(glsm_fluid f, int iter) {
     glsm_coupler c = f->c;
     MarkerArgs m{c->d_gels, c->mk, f->F.c[f->cur], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 0};
     CK(launch_conc_markers(m, c->stream));
-    ConcArgs a{f->F, c->mk, c->d_ctl, (int)c->gels.size(), f->cur, 0};
+    ConcArgs a{f->F, c->mk, c->d_ctl, (int)c->gels.size(), f->cur, 0, make_fastdiv((unsigned)f->F.nx),
+               make_fastdiv((unsigned)(f->F.nx * f->F.ny))};
     CK(launch_conv_diff(a, c->stream));
     f->cur ^= 1;
     return GLSM_OK;
@@ -923,7 +927,8 @@ static int enqueue_iteration(glsm_fluid f, int iter_arg, int p0, int cur) {
     CK(cudaEventRecord(c->ev_join, c->side));
     for (int k = 0; k < nsub; k++) CK(launch_substep(step_args(f, k, iter_arg), (p0 + k) & 1, s));
     CK(cudaStreamWaitEvent(s, c->ev_join, 0));
-    ConcArgs a{f->F, c->mk, c->d_ctl, (int)c->gels.size(), cur, iter_arg < 0 ? 1 : 0};
+    ConcArgs a{f->F, c->mk, c->d_ctl, (int)c->gels.size(), cur, iter_arg < 0 ? 1 : 0,
+               make_fastdiv((unsigned)f->F.nx), make_fastdiv((unsigned)(f->F.nx * f->F.ny))};
     CK(launch_conv_diff(a, s));
     return GLSM_OK;
 }
@@ -992,6 +997,30 @@ int glsm_fluid_sync(glsm_fluid f) {
                     (err & kErrNonFinite) ? " [non-finite gel state]" : "");
     }
     return GLSM_OK;
+}
+
+// Fluid::stepVelocity with a CUDA event pair around every substep launch on the
+// system stream; ms[k] receives the duration of substep k (for the roofline)
+int glsm_fluid_profile_velocity(glsm_fluid f, int iter, float* ms) {
+    if (!f || !ms || iter < 0) return fail(GLSM_ERR_ARG, "bad argument");
+    cudaStream_t s = f->c->stream;
+    const int nsub = f->F.nsub;
+    const int p0 = (int)(f->substeps & 1);
+    std::vector<cudaEvent_t> ev(2 * (size_t)nsub, nullptr);
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    CK(cudaMemsetAsync(f->d_sync, 0, 2 * sizeof(unsigned) * nsub, s));
+    int r = GLSM_OK;
+    for (int k = 0; k < nsub && r == GLSM_OK; k++) {
+        CK(cudaEventRecord(ev[2 * k], s));
+        cudaError_t e = launch_substep(step_args(f, k, iter), (p0 + k) & 1, s);
+        if (e != cudaSuccess) r = fail(GLSM_ERR_CUDA, "substep launch: %s", cudaGetErrorString(e));
+        CK(cudaEventRecord(ev[2 * k + 1], s));
+    }
+    f->substeps += nsub;
+    CK(cudaStreamSynchronize(s));
+    for (int k = 0; k < nsub && r == GLSM_OK; k++) CK(cudaEventElapsedTime(&ms[k], ev[2 * k], ev[2 * k + 1]));
+    for (auto& e : ev) cudaEventDestroy(e);
+    return r;
 }
 
 static int ensure_scratch(glsm_fluid f) {

@@ -17,6 +17,7 @@
 #include <cuda_fp16.h>
 
 #include "d3q19.cuh"
+#include "fastdiv.h"
 #include "glsm_internal.h"
 #include "lbm.h"
 
@@ -73,8 +74,8 @@ __device__ __forceinline__ float warp_sum(float v) {
 struct TileExt {
     int x0, x1, y0, y1, z0, z1;
 };
-__device__ __forceinline__ TileExt tile_extent(long long c0, long long c1, int nx, int ny) {
-    const long long nxy = (long long)nx * ny;
+__device__ __forceinline__ TileExt tile_extent(unsigned c0, unsigned c1, unsigned nx, unsigned ny) {
+    const unsigned nxy = nx * ny;
     TileExt e;
     e.z0 = (int)(c0 / nxy);
     e.z1 = (int)(c1 / nxy);
@@ -85,15 +86,15 @@ __device__ __forceinline__ TileExt tile_extent(long long c0, long long c1, int n
         e.x1 = nx - 1;
         return e;
     }
-    long long r0 = c0 - (long long)e.z0 * nxy, r1 = c1 - (long long)e.z0 * nxy;
+    const unsigned r0 = c0 - (unsigned)e.z0 * nxy, r1 = c1 - (unsigned)e.z0 * nxy;
     e.y0 = (int)(r0 / nx);
     e.y1 = (int)(r1 / nx);
     if (e.y0 != e.y1) {
         e.x0 = 0;
         e.x1 = nx - 1;
     } else {
-        e.x0 = (int)(r0 - (long long)e.y0 * nx);
-        e.x1 = (int)(r1 - (long long)e.y0 * nx);
+        e.x0 = (int)(r0 - (unsigned)e.y0 * nx);
+        e.x1 = (int)(r1 - (unsigned)e.y0 * nx);
     }
     return e;
 }
@@ -205,8 +206,53 @@ __device__ __forceinline__ void wait_ibm(const StepArgs& a) {
 // ---------------------------------------------------------------------------
 // the substep kernel
 // ---------------------------------------------------------------------------
-template <int ST, int PARITY>
-__global__ void __launch_bounds__(kTile) lbm_substep_kernel(StepArgs a) {
+// BGK collision with Guo forcing in deviation form, pairing each direction q
+// with opp(q): the equilibrium and forcing terms split into parts even and odd
+// in c_q, shared by the pair.  d_q <- d_q + omega (deq_q - d_q) + F_q with
+//   deq_q = w_q (drho + rho (3 cu + 4.5 cu^2 - 1.5 uu))
+//   F_q   = w_q (1 - 1/(2 tau)) (3 cF + 9 cu cF - 3 uF)
+__device__ __forceinline__ void collide(float (&d)[19], float Fx, float Fy, float Fz, float omega, float fp,
+                                        float& ux, float& uy, float& uz, float& rho) {
+    float drho = d[0], jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int q = 1; q < 19; q++) {
+        if (qopp(q) < q) continue;  // visit each pair once, through its first member
+        const int o = qopp(q);
+        const float sum = d[q] + d[o], dif = d[q] - d[o];
+        drho += sum;
+        if (qcx(q)) jx += qcx(q) > 0 ? dif : -dif;
+        if (qcy(q)) jy += qcy(q) > 0 ? dif : -dif;
+        if (qcz(q)) jz += qcz(q) > 0 ? dif : -dif;
+    }
+    rho = 1.0f + drho;
+    const float inv = 1.0f / rho;
+    ux = (jx + 0.5f * Fx) * inv;
+    uy = (jy + 0.5f * Fy) * inv;
+    uz = (jz + 0.5f * Fz) * inv;
+    const float uu = ux * ux + uy * uy + uz * uz;
+    const float uF = ux * Fx + uy * Fy + uz * Fz;
+    const float even0 = drho - 1.5f * rho * uu;  // deq / w without the cu terms
+    const float force0 = -3.0f * fp * uF;         // F / w without the c terms
+    d[0] += omega * (qw(0) * even0 - d[0]) + qw(0) * force0;
+#pragma unroll
+    for (int q = 1; q < 19; q++) {
+        if (qopp(q) < q) continue;
+        const int o = qopp(q);
+        const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
+        const float cu = (cx ? (cx > 0 ? ux : -ux) : 0.f) + (cy ? (cy > 0 ? uy : -uy) : 0.f) +
+                         (cz ? (cz > 0 ? uz : -uz) : 0.f);
+        const float cF = (cx ? (cx > 0 ? Fx : -Fx) : 0.f) + (cy ? (cy > 0 ? Fy : -Fy) : 0.f) +
+                         (cz ? (cz > 0 ? Fz : -Fz) : 0.f);
+        const float w = qw(q);
+        const float ev = even0 + 4.5f * rho * cu * cu, od = 3.0f * rho * cu;
+        const float fe = force0 + 9.0f * fp * cu * cF, fo = 3.0f * fp * cF;
+        d[q] += omega * (w * (ev + od) - d[q]) + w * (fe + fo);
+        d[o] += omega * (w * (ev - od) - d[o]) + w * (fe - fo);
+    }
+}
+
+template <int ST, int PARITY, int PERX>
+__global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
     using IO = PopIO<ST>;
     using T = typename IO::T;
     __shared__ unsigned s_ticket;
@@ -223,78 +269,79 @@ __global__ void __launch_bounds__(kTile) lbm_substep_kernel(StepArgs a) {
         return;
     }
     const FluidDev& F = a.F;
-    const int nx = F.nx, ny = F.ny, nz = F.nz;
-    const long long N = F.N, S = F.S, nxy = (long long)nx * ny;
-    const long long c0 = (long long)(t - a.n_ibm) * kTile;
+    const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
+    const unsigned N = (unsigned)F.N, S = (unsigned)F.S, nxy = nx * ny;
+    const unsigned c0 = (t - a.n_ibm) * kTile;
     if (c0 >= N) return;  // surplus CTA (never launched by the host; kept for safety)
-    const long long c1 = min(c0 + kTile - 1, N - 1);
+    const unsigned c1 = min(c0 + kTile - 1, N - 1);
     const TileExt ext = tile_extent(c0, c1, nx, ny);
     const int nb = tile_boxes(a.Mk.boxes, a.n_boxes, ext, s_b, &s_nb);
     if (nb > 0) wait_ibm(a);
 
-    const long long i = c0 + threadIdx.x;
+    const unsigned i = c0 + threadIdx.x;
     if (i > c1) return;
-    const int z = (int)(i / nxy);
-    const long long rem = i - (long long)z * nxy;
-    const int y = (int)(rem / nx);
-    const int x = (int)(rem - (long long)y * nx);
+    const unsigned z = fdiv(i, a.div_nxy);
+    const unsigned rem = i - z * nxy;
+    const unsigned y = fdiv(rem, a.div_nx);
+    const unsigned x = rem - y * nx;
 
     bool inb = false;
-    for (int j = 0; j < nb; j++) inb |= inside(s_b[j], x, y, z);
-
-    // neighbour offsets and wall flags per axis (m: minus side, p: plus side)
-    long long mo[3], po[3];
-    bool mw[3], pw[3];
-    {
-        const int c[3] = {x, y, z};
-        const int n[3] = {nx, ny, nz};
-        const long long st[3] = {1, nx, nxy};
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            mw[d] = false;
-            pw[d] = false;
-            if (c[d] > 0)
-                mo[d] = -st[d];
-            else if (F.per[d])
-                mo[d] = (long long)(n[d] - 1) * st[d];
-            else {
-                mo[d] = 0;
-                mw[d] = true;
-            }
-            if (c[d] < n[d] - 1)
-                po[d] = st[d];
-            else if (F.per[d])
-                po[d] = -(long long)(n[d] - 1) * st[d];
-            else {
-                po[d] = 0;
-                pw[d] = true;
-            }
-        }
-    }
+    for (int j = 0; j < nb; j++) inb |= inside(s_b[j], (int)x, (int)y, (int)z);
 
     T* P = reinterpret_cast<T*>(F.pop);
+    const float isc = F.inv_scale;
     float d[19];
+    // odd substeps: a warp whose cells are all off the y and z boundary planes
+    // streams with constant neighbour offsets (x walls or wraps per lane);
+    // other warps take the general path
+    bool fast = true;
+    if (PARITY == 1) fast = __all_sync(__activemask(), (y - 1u < ny - 2u) && (z - 1u < nz - 2u));
     if (PARITY == 0) {
 #pragma unroll
-        for (int q = 0; q < 19; q++) d[q] = IO::ld(P + (long long)q * S + i, F.inv_scale);
-    } else {
+        for (int q = 0; q < 19; q++) d[q] = IO::ld(P + q * S + i, isc);
+    } else if (fast) {
 #pragma unroll
         for (int q = 0; q < 19; q++) {
-            // arriving population f_q(x) = post-collision f_q(x - c_q), stored in
-            // slot opp(q) at x - c_q; across a wall it is the bounced opp(q)
-            // population of x itself, stored in slot q at x
+            // arriving f_q(x) = post-collision f_q(x - c_q), in slot opp(q) at x - c_q;
+            // across a wall it is the bounced opp(q) population of x, in slot q at x
+            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
+            const unsigned nbr = i - (unsigned)(cx + cy * (int)nx + cz * (int)nxy);
+            if (cx == 0) {
+                d[q] = IO::ld(P + qopp(q) * S + nbr, isc);
+            } else {
+                const bool edge = (cx > 0) ? (x == 0) : (x == nx - 1);
+                if (PERX)
+                    d[q] = IO::ld(P + qopp(q) * S + (edge ? nbr + (unsigned)(cx * (int)nx) : nbr), isc);
+                else
+                    d[q] = IO::ld(P + (edge ? q * S + i : qopp(q) * S + nbr), isc);
+            }
+        }
+    } else {
+        int mo[3], po[3];
+        bool mw[3], pw[3];
+        const unsigned c[3] = {x, y, z}, n[3] = {nx, ny, nz}, st[3] = {1u, nx, nxy};
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            mw[k] = pw[k] = false;
+            mo[k] = -(int)st[k];
+            po[k] = (int)st[k];
+            if (c[k] == 0) {
+                if (F.per[k]) mo[k] = (int)((n[k] - 1) * st[k]);
+                else mw[k] = true;
+            }
+            if (c[k] == n[k] - 1) {
+                if (F.per[k]) po[k] = -(int)((n[k] - 1) * st[k]);
+                else pw[k] = true;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
             const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
             const bool wall = (cx > 0 && mw[0]) || (cx < 0 && pw[0]) || (cy > 0 && mw[1]) || (cy < 0 && pw[1]) ||
                               (cz > 0 && mw[2]) || (cz < 0 && pw[2]);
-            long long off = 0;
-            if (cx > 0) off += mo[0];
-            if (cx < 0) off += po[0];
-            if (cy > 0) off += mo[1];
-            if (cy < 0) off += po[1];
-            if (cz > 0) off += mo[2];
-            if (cz < 0) off += po[2];
-            const long long src = wall ? (long long)q * S + i : (long long)qopp(q) * S + i + off;
-            d[q] = IO::ld(P + src, F.inv_scale);
+            const int off = (cx > 0 ? mo[0] : cx < 0 ? po[0] : 0) + (cy > 0 ? mo[1] : cy < 0 ? po[1] : 0) +
+                            (cz > 0 ? mo[2] : cz < 0 ? po[2] : 0);
+            d[q] = IO::ld(P + (wall ? q * S + i : qopp(q) * S + i + (unsigned)off), isc);
         }
     }
 
@@ -307,54 +354,56 @@ __global__ void __launch_bounds__(kTile) lbm_substep_kernel(StepArgs a) {
         Fz += fi.z;
         __stcg(&F.Fibm[i], make_float4(0.f, 0.f, 0.f, 0.f));
     }
+    float ux, uy, uz, rho;
+    collide(d, Fx, Fy, Fz, F.omega, F.fpref, ux, uy, uz, rho);
 
-    // moments (k_macros) and BGK + Guo forcing (k_collide) in deviation form
-    float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
-#pragma unroll
-    for (int q = 0; q < 19; q++) {
-        drho += d[q];
-        if (qcx(q) > 0) jx += d[q];
-        if (qcx(q) < 0) jx -= d[q];
-        if (qcy(q) > 0) jy += d[q];
-        if (qcy(q) < 0) jy -= d[q];
-        if (qcz(q) > 0) jz += d[q];
-        if (qcz(q) < 0) jz -= d[q];
-    }
-    const float rho = 1.0f + drho;
-    const float ux = (jx + 0.5f * Fx) / rho, uy = (jy + 0.5f * Fy) / rho, uz = (jz + 0.5f * Fz) / rho;
-    const float uu = ux * ux + uy * uy + uz * uz;
-    const float uF = ux * Fx + uy * Fy + uz * Fz;
-    const float omega = F.omega, fp = F.fpref;
-#pragma unroll
-    for (int q = 0; q < 19; q++) {
-        const float cx = (float)qcx(q), cy = (float)qcy(q), cz = (float)qcz(q);
-        const float cu = cx * ux + cy * uy + cz * uz;
-        const float cF = cx * Fx + cy * Fy + cz * Fz;
-        const float deq = qw(q) * (drho + rho * (3.0f * cu + 4.5f * cu * cu - 1.5f * uu));
-        const float Ft = qw(q) * fp * (3.0f * cF + 9.0f * cu * cF - 3.0f * uF);
-        d[q] = d[q] - omega * (d[q] - deq) + Ft;
-    }
-
+    const float sc = F.scale;
     if (PARITY == 0) {
 #pragma unroll
-        for (int q = 0; q < 19; q++) IO::st(P + (long long)qopp(q) * S + i, d[q], F.scale);
-    } else {
+        for (int q = 0; q < 19; q++) IO::st(P + qopp(q) * S + i, d[q], sc);
+    } else if (fast) {
 #pragma unroll
         for (int q = 0; q < 19; q++) {
             // post-collision f_q(x) streams to x + c_q (slot q), or bounces back
             // into slot opp(q) of x when x + c_q lies beyond a wall
             const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
+            const unsigned nbr = i + (unsigned)(cx + cy * (int)nx + cz * (int)nxy);
+            if (cx == 0) {
+                IO::st(P + q * S + nbr, d[q], sc);
+            } else {
+                const bool edge = (cx > 0) ? (x == nx - 1) : (x == 0);
+                if (PERX)
+                    IO::st(P + q * S + (edge ? nbr - (unsigned)(cx * (int)nx) : nbr), d[q], sc);
+                else
+                    IO::st(P + (edge ? qopp(q) * S + i : q * S + nbr), d[q], sc);
+            }
+        }
+    } else {
+        int mo[3], po[3];
+        bool mw[3], pw[3];
+        const unsigned c[3] = {x, y, z}, n[3] = {nx, ny, nz}, st[3] = {1u, nx, nxy};
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            mw[k] = pw[k] = false;
+            mo[k] = -(int)st[k];
+            po[k] = (int)st[k];
+            if (c[k] == 0) {
+                if (F.per[k]) mo[k] = (int)((n[k] - 1) * st[k]);
+                else mw[k] = true;
+            }
+            if (c[k] == n[k] - 1) {
+                if (F.per[k]) po[k] = -(int)((n[k] - 1) * st[k]);
+                else pw[k] = true;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
             const bool wall = (cx > 0 && pw[0]) || (cx < 0 && mw[0]) || (cy > 0 && pw[1]) || (cy < 0 && mw[1]) ||
                               (cz > 0 && pw[2]) || (cz < 0 && mw[2]);
-            long long off = 0;
-            if (cx > 0) off += po[0];
-            if (cx < 0) off += mo[0];
-            if (cy > 0) off += po[1];
-            if (cy < 0) off += mo[1];
-            if (cz > 0) off += po[2];
-            if (cz < 0) off += mo[2];
-            const long long dst = wall ? (long long)qopp(q) * S + i : (long long)q * S + i + off;
-            IO::st(P + dst, d[q], F.scale);
+            const int off = (cx > 0 ? po[0] : cx < 0 ? mo[0] : 0) + (cy > 0 ? po[1] : cy < 0 ? mo[1] : 0) +
+                            (cz > 0 ? po[2] : cz < 0 ? mo[2] : 0);
+            IO::st(P + (wall ? qopp(q) * S + i : q * S + i + (unsigned)off), d[q], sc);
         }
     }
     if (inb || a.last) F.u[i] = make_float4(ux, uy, uz, rho);
@@ -372,31 +421,31 @@ __global__ void __launch_bounds__(kTile) conv_diff_kernel(ConcArgs a) {
     }
     __syncthreads();
     const FluidDev& F = a.F;
-    const int nx = F.nx, ny = F.ny, nz = F.nz;
-    const long long N = F.N, nxy = (long long)nx * ny;
-    const long long c0 = (long long)blockIdx.x * kTile;
-    const long long c1 = min(c0 + kTile - 1, N - 1);
+    const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
+    const unsigned N = (unsigned)F.N, nxy = nx * ny;
+    const unsigned c0 = blockIdx.x * kTile;
+    const unsigned c1 = min(c0 + kTile - 1, N - 1);
     const TileExt ext = tile_extent(c0, c1, nx, ny);
     const int nb = tile_boxes(a.Mk.boxes, a.n_boxes, ext, s_b, &s_nb);
-    const long long i = c0 + threadIdx.x;
+    const unsigned i = c0 + threadIdx.x;
     if (i > c1) return;
-    const int z = (int)(i / nxy);
-    const long long rem = i - (long long)z * nxy;
-    const int y = (int)(rem / nx);
-    const int x = (int)(rem - (long long)y * nx);
+    const unsigned z = fdiv(i, a.div_nxy);
+    const unsigned rem = i - z * nxy;
+    const unsigned y = fdiv(rem, a.div_nx);
+    const unsigned x = rem - y * nx;
     bool inb = false;
-    for (int j = 0; j < nb; j++) inb |= inside(s_b[j], x, y, z);
+    for (int j = 0; j < nb; j++) inb |= inside(s_b[j], (int)x, (int)y, (int)z);
 
-    const int xp = (x + 1 < nx) ? x + 1 : (F.per[0] ? 0 : x);
-    const int xm = (x - 1 >= 0) ? x - 1 : (F.per[0] ? nx - 1 : x);
-    const int yp = (y + 1 < ny) ? y + 1 : (F.per[1] ? 0 : y);
-    const int ym = (y - 1 >= 0) ? y - 1 : (F.per[1] ? ny - 1 : y);
-    const int zp = (z + 1 < nz) ? z + 1 : (F.per[2] ? 0 : z);
-    const int zm = (z - 1 >= 0) ? z - 1 : (F.per[2] ? nz - 1 : z);
-    const long long base = (long long)z * nxy + (long long)y * nx;
-    const long long ixp = base + xp, ixm = base + xm;
-    const long long iyp = (long long)z * nxy + (long long)yp * nx + x, iym = (long long)z * nxy + (long long)ym * nx + x;
-    const long long izp = (long long)zp * nxy + (long long)y * nx + x, izm = (long long)zm * nxy + (long long)y * nx + x;
+    const unsigned xp = (x + 1 < nx) ? x + 1 : (F.per[0] ? 0 : x);
+    const unsigned xm = (x >= 1) ? x - 1 : (F.per[0] ? nx - 1 : x);
+    const unsigned yp = (y + 1 < ny) ? y + 1 : (F.per[1] ? 0 : y);
+    const unsigned ym = (y >= 1) ? y - 1 : (F.per[1] ? ny - 1 : y);
+    const unsigned zp = (z + 1 < nz) ? z + 1 : (F.per[2] ? 0 : z);
+    const unsigned zm = (z >= 1) ? z - 1 : (F.per[2] ? nz - 1 : z);
+    const unsigned base = z * nxy + y * nx;
+    const unsigned ixp = base + xp, ixm = base + xm;
+    const unsigned iyp = z * nxy + yp * nx + x, iym = z * nxy + ym * nx + x;
+    const unsigned izp = zp * nxy + y * nx + x, izm = zm * nxy + y * nx + x;
 
     const float* c1p = F.c[a.cur];
     float* c2p = F.c[a.cur ^ 1];
@@ -474,10 +523,12 @@ int lbm_grid(const StepArgs& a) {
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
     dim3 grid(lbm_grid(a)), block(kTile);
 #define GLSM_SUB(ST)                                                           \
-    if (parity)                                                                \
-        lbm_substep_kernel<ST, 1><<<grid, block, 0, s>>>(a);                   \
+    if (parity && a.F.per[0])                                                  \
+        lbm_substep_kernel<ST, 1, 1><<<grid, block, 0, s>>>(a);                \
+    else if (parity)                                                           \
+        lbm_substep_kernel<ST, 1, 0><<<grid, block, 0, s>>>(a);                \
     else                                                                       \
-        lbm_substep_kernel<ST, 0><<<grid, block, 0, s>>>(a);
+        lbm_substep_kernel<ST, 0, 0><<<grid, block, 0, s>>>(a);
     switch (a.F.storage) {
         case kStoreF32: GLSM_SUB(kStoreF32); break;
         case kStoreF16: GLSM_SUB(kStoreF16); break;

@@ -1,5 +1,6 @@
 // lbm.h -- launch arguments and launchers of the fluid kernels (lbm.cu)
 #pragma once
+#include "fastdiv.h"
 #include "glsm_internal.h"
 
 namespace glsm {
@@ -15,6 +16,7 @@ struct StepArgs {
     int iter_arg;        // >= 0: iteration number; < 0: read Ctl::iter
     int k;               // substep index within the iteration
     int last;            // k == nsub - 1: write u for every cell
+    FastDiv div_nx, div_nxy;
 };
 
 struct ConcArgs {
@@ -24,6 +26,7 @@ struct ConcArgs {
     int n_boxes;
     int cur;        // index of the current concentration buffer
     int bump_iter;  // advance Ctl::iter (graph mode)
+    FastDiv div_nx, div_nxy;
 };
 
 int lbm_grid(const StepArgs& a);

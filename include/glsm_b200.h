@@ -74,7 +74,7 @@ enum glsm_gel_field {
 /* lattice fields for glsm_fluid_read / _write (FP32, reference layout) */
 enum glsm_fluid_field {
     GLSM_FLUID_POP = 0, /* d_f after the last substep: 19*N absolute populations */
-    GLSM_FLUID_RHO = 1, /* d_rho: N (computed from the populations)              */
+    GLSM_FLUID_RHO = 1, /* d_rho: N, density moment of the last substep's macros  */
     GLSM_FLUID_U = 2,   /* d_u: 3*N, velocity of the last substep's macros       */
     GLSM_FLUID_C1 = 3   /* d_c1: N, concentration                                */
 };
@@ -193,6 +193,10 @@ int glsm_fluid_read(glsm_fluid f, int field, float* dst, size_t count);
 int glsm_fluid_write(glsm_fluid f, int field, const float* src, size_t count);
 /* nx, ny, nz, N, nsub, storage, device bytes, substeps done */
 int glsm_fluid_info(glsm_fluid f, int64_t out[8]);
+/* Fluid::stepVelocity(iter) with a CUDA event pair around each substep launch on
+ * the system stream; ms[k] (nsub floats) receives the duration of substep k.
+ * Used to report the substep kernel's achieved bandwidth. */
+int glsm_fluid_profile_velocity(glsm_fluid f, int iter, float* ms);
 /* gel_to_lbm_vel and lbm_to_gel_vel (src/fluid.cu:221-222) */
 int glsm_fluid_units(glsm_fluid f, float out[2]);
 
