@@ -82,6 +82,7 @@ struct glsm_fluid_s {
     int cur = 0;                 // current concentration buffer
     long long substeps = 0;      // AA parity bookkeeping
     float* scratch = nullptr;    // 19*N floats, allocated on first use
+    int lbm_ctas = 0;            // resident CTAs of the persistent substep kernel
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 };
 
@@ -760,6 +761,8 @@ static StepArgs step_args(glsm_fluid f, int k, int iter_arg) {
     a.last = (k == f->F.nsub - 1);
     a.div_nx = make_fastdiv((unsigned)f->F.nx);
     a.div_nxy = make_fastdiv((unsigned)(f->F.nx * f->F.ny));
+    a.n_tiles = (int)((f->F.N + kTileCells - 1) / kTileCells);
+    a.lbm_ctas = f->lbm_ctas;
     return a;
 }
 
@@ -837,6 +840,7 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     }
     int nsub_phys;
     fluid_units(d->tau, d->h, c->g2l, c->l2g, nsub_phys);
+    f->lbm_ctas = lbm_resident_ctas();
     f->c = c;
     c->fluid = f;
     // the gels' gather now knows the lattice

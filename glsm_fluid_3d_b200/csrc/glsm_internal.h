@@ -9,7 +9,9 @@
 
 namespace glsm {
 
-constexpr int kTile = 256;        // lattice cells per LBM CTA (one cell per thread)
+constexpr int kTile = 256;        // threads of an LBM CTA
+constexpr int kCellsPerThread = 2;
+constexpr int kTileCells = kTile * kCellsPerThread;  // lattice cells per LBM ticket
 constexpr int kMarkersPerTask = 8;  // IBM task CTA: one warp per marker
 constexpr int kMaxBoxes = 64;     // force-region boxes (one per gel) seen by one LBM launch
 constexpr int kGelThreads = 512;  // threads of the one-CTA-per-gel kernel

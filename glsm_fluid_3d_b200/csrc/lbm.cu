@@ -74,11 +74,12 @@ __device__ __forceinline__ float warp_sum(float v) {
 struct TileExt {
     int x0, x1, y0, y1, z0, z1;
 };
-__device__ __forceinline__ TileExt tile_extent(unsigned c0, unsigned c1, unsigned nx, unsigned ny) {
+__device__ __forceinline__ TileExt tile_extent(unsigned c0, unsigned c1, unsigned nx, unsigned ny,
+                                               const FastDiv& dnx, const FastDiv& dnxy) {
     const unsigned nxy = nx * ny;
     TileExt e;
-    e.z0 = (int)(c0 / nxy);
-    e.z1 = (int)(c1 / nxy);
+    e.z0 = (int)fdiv(c0, dnxy);
+    e.z1 = (int)fdiv(c1, dnxy);
     if (e.z0 != e.z1) {
         e.y0 = 0;
         e.y1 = ny - 1;
@@ -87,8 +88,8 @@ __device__ __forceinline__ TileExt tile_extent(unsigned c0, unsigned c1, unsigne
         return e;
     }
     const unsigned r0 = c0 - (unsigned)e.z0 * nxy, r1 = c1 - (unsigned)e.z0 * nxy;
-    e.y0 = (int)(r0 / nx);
-    e.y1 = (int)(r1 / nx);
+    e.y0 = (int)fdiv(r0, dnx);
+    e.y1 = (int)fdiv(r1, dnx);
     if (e.y0 != e.y1) {
         e.x0 = 0;
         e.x1 = nx - 1;
@@ -206,88 +207,112 @@ __device__ __forceinline__ void wait_ibm(const StepArgs& a) {
 // ---------------------------------------------------------------------------
 // the substep kernel
 // ---------------------------------------------------------------------------
-// BGK collision with Guo forcing in deviation form, pairing each direction q
-// with opp(q): the equilibrium and forcing terms split into parts even and odd
-// in c_q, shared by the pair.  d_q <- d_q + omega (deq_q - d_q) + F_q with
+template <int C>
+__device__ __forceinline__ float sgn(float v) {
+    return C > 0 ? v : -v;
+}
+// c . v for a D3Q19 direction (at most two non-zero components), without
+// adding IEEE zeros that the compiler could not fold away
+template <int CX, int CY, int CZ>
+__device__ __forceinline__ float cdot(float x, float y, float z) {
+    if constexpr (CX != 0 && CY != 0) return sgn<CX>(x) + sgn<CY>(y);
+    else if constexpr (CX != 0 && CZ != 0) return sgn<CX>(x) + sgn<CZ>(z);
+    else if constexpr (CY != 0 && CZ != 0) return sgn<CY>(y) + sgn<CZ>(z);
+    else if constexpr (CX != 0) return sgn<CX>(x);
+    else if constexpr (CY != 0) return sgn<CY>(y);
+    else return sgn<CZ>(z);
+}
+
+struct CollideTerms {
+    float ux, uy, uz, Fx, Fy, Fz, even0, force0, rho45, rho3, fp9, fp3, omega;
+};
+
+// relaxation of the pair (Q, opp(Q)): equilibrium and forcing split into the
+// parts even and odd in c_Q, shared by the pair
+template <int Q>
+__device__ __forceinline__ void collide_pair(float (&d)[19], const CollideTerms& t) {
+    constexpr int O = qopp(Q);
+    constexpr float w = qw(Q);
+    const float cu = cdot<qcx(Q), qcy(Q), qcz(Q)>(t.ux, t.uy, t.uz);
+    const float cF = cdot<qcx(Q), qcy(Q), qcz(Q)>(t.Fx, t.Fy, t.Fz);
+    const float ev = fmaf(t.rho45 * cu, cu, t.even0), od = t.rho3 * cu;
+    const float fe = fmaf(t.fp9 * cu, cF, t.force0), fo = t.fp3 * cF;
+    d[Q] = fmaf(t.omega, fmaf(w, ev + od, -d[Q]), fmaf(w, fe + fo, d[Q]));
+    d[O] = fmaf(t.omega, fmaf(w, ev - od, -d[O]), fmaf(w, fe - fo, d[O]));
+}
+
+template <int Q>
+__device__ __forceinline__ void moment_pair(const float (&d)[19], float& drho, float& jx, float& jy, float& jz) {
+    constexpr int O = qopp(Q);
+    const float sum = d[Q] + d[O], dif = d[Q] - d[O];
+    drho += sum;
+    if constexpr (qcx(Q) != 0) jx += sgn<qcx(Q)>(dif);
+    if constexpr (qcy(Q) != 0) jy += sgn<qcy(Q)>(dif);
+    if constexpr (qcz(Q) != 0) jz += sgn<qcz(Q)>(dif);
+}
+
+// BGK collision with Guo forcing in deviation form:
+// d_q <- d_q + omega (deq_q - d_q) + F_q with
 //   deq_q = w_q (drho + rho (3 cu + 4.5 cu^2 - 1.5 uu))
 //   F_q   = w_q (1 - 1/(2 tau)) (3 cF + 9 cu cF - 3 uF)
+// The first members of the nine (q, opp q) pairs: 1 3 5 7 8 11 12 15 16.
 __device__ __forceinline__ void collide(float (&d)[19], float Fx, float Fy, float Fz, float omega, float fp,
                                         float& ux, float& uy, float& uz, float& rho) {
     float drho = d[0], jx = 0.f, jy = 0.f, jz = 0.f;
-#pragma unroll
-    for (int q = 1; q < 19; q++) {
-        if (qopp(q) < q) continue;  // visit each pair once, through its first member
-        const int o = qopp(q);
-        const float sum = d[q] + d[o], dif = d[q] - d[o];
-        drho += sum;
-        if (qcx(q)) jx += qcx(q) > 0 ? dif : -dif;
-        if (qcy(q)) jy += qcy(q) > 0 ? dif : -dif;
-        if (qcz(q)) jz += qcz(q) > 0 ? dif : -dif;
-    }
+    moment_pair<1>(d, drho, jx, jy, jz);
+    moment_pair<3>(d, drho, jx, jy, jz);
+    moment_pair<5>(d, drho, jx, jy, jz);
+    moment_pair<7>(d, drho, jx, jy, jz);
+    moment_pair<8>(d, drho, jx, jy, jz);
+    moment_pair<11>(d, drho, jx, jy, jz);
+    moment_pair<12>(d, drho, jx, jy, jz);
+    moment_pair<15>(d, drho, jx, jy, jz);
+    moment_pair<16>(d, drho, jx, jy, jz);
     rho = 1.0f + drho;
-    const float inv = 1.0f / rho;
+    const float inv = __frcp_rn(rho);
     ux = (jx + 0.5f * Fx) * inv;
     uy = (jy + 0.5f * Fy) * inv;
     uz = (jz + 0.5f * Fz) * inv;
     const float uu = ux * ux + uy * uy + uz * uz;
     const float uF = ux * Fx + uy * Fy + uz * Fz;
-    const float even0 = drho - 1.5f * rho * uu;  // deq / w without the cu terms
-    const float force0 = -3.0f * fp * uF;         // F / w without the c terms
-    d[0] += omega * (qw(0) * even0 - d[0]) + qw(0) * force0;
-#pragma unroll
-    for (int q = 1; q < 19; q++) {
-        if (qopp(q) < q) continue;
-        const int o = qopp(q);
-        const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
-        const float cu = (cx ? (cx > 0 ? ux : -ux) : 0.f) + (cy ? (cy > 0 ? uy : -uy) : 0.f) +
-                         (cz ? (cz > 0 ? uz : -uz) : 0.f);
-        const float cF = (cx ? (cx > 0 ? Fx : -Fx) : 0.f) + (cy ? (cy > 0 ? Fy : -Fy) : 0.f) +
-                         (cz ? (cz > 0 ? Fz : -Fz) : 0.f);
-        const float w = qw(q);
-        const float ev = even0 + 4.5f * rho * cu * cu, od = 3.0f * rho * cu;
-        const float fe = force0 + 9.0f * fp * cu * cF, fo = 3.0f * fp * cF;
-        d[q] += omega * (w * (ev + od) - d[q]) + w * (fe + fo);
-        d[o] += omega * (w * (ev - od) - d[o]) + w * (fe - fo);
-    }
+    CollideTerms t;
+    t.ux = ux;
+    t.uy = uy;
+    t.uz = uz;
+    t.Fx = Fx;
+    t.Fy = Fy;
+    t.Fz = Fz;
+    t.even0 = drho - 1.5f * rho * uu;  // deq / w without the c terms
+    t.force0 = -3.0f * fp * uF;         // F / w without the c terms
+    t.rho45 = 4.5f * rho;
+    t.rho3 = 3.0f * rho;
+    t.fp9 = 9.0f * fp;
+    t.fp3 = 3.0f * fp;
+    t.omega = omega;
+    d[0] = fmaf(omega, fmaf(qw(0), t.even0, -d[0]), fmaf(qw(0), t.force0, d[0]));
+    collide_pair<1>(d, t);
+    collide_pair<3>(d, t);
+    collide_pair<5>(d, t);
+    collide_pair<7>(d, t);
+    collide_pair<8>(d, t);
+    collide_pair<11>(d, t);
+    collide_pair<12>(d, t);
+    collide_pair<15>(d, t);
+    collide_pair<16>(d, t);
 }
 
+// one cell of a substep: gather (AA pattern), collide, scatter
 template <int ST, int PARITY, int PERX>
-__global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
+__device__ __forceinline__ void lbm_cell(const StepArgs& a, unsigned i, bool inb) {
     using IO = PopIO<ST>;
     using T = typename IO::T;
-    __shared__ unsigned s_ticket;
-    __shared__ int s_nb;
-    __shared__ Box s_b[kMaxBoxes];
-    if (threadIdx.x == 0) {
-        s_ticket = atomicAdd(&a.tickets[a.k], 1u);
-        s_nb = 0;
-    }
-    __syncthreads();
-    const unsigned t = s_ticket;
-    if (t < (unsigned)a.n_ibm) {
-        ibm_task(a, t);
-        return;
-    }
     const FluidDev& F = a.F;
     const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
-    const unsigned N = (unsigned)F.N, S = (unsigned)F.S, nxy = nx * ny;
-    const unsigned c0 = (t - a.n_ibm) * kTile;
-    if (c0 >= N) return;  // surplus CTA (never launched by the host; kept for safety)
-    const unsigned c1 = min(c0 + kTile - 1, N - 1);
-    const TileExt ext = tile_extent(c0, c1, nx, ny);
-    const int nb = tile_boxes(a.Mk.boxes, a.n_boxes, ext, s_b, &s_nb);
-    if (nb > 0) wait_ibm(a);
-
-    const unsigned i = c0 + threadIdx.x;
-    if (i > c1) return;
+    const unsigned S = (unsigned)F.S, nxy = nx * ny;
     const unsigned z = fdiv(i, a.div_nxy);
     const unsigned rem = i - z * nxy;
     const unsigned y = fdiv(rem, a.div_nx);
     const unsigned x = rem - y * nx;
-
-    bool inb = false;
-    for (int j = 0; j < nb; j++) inb |= inside(s_b[j], (int)x, (int)y, (int)z);
-
     T* P = reinterpret_cast<T*>(F.pop);
     const float isc = F.inv_scale;
     float d[19];
@@ -298,7 +323,7 @@ __global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
     if (PARITY == 1) fast = __all_sync(__activemask(), (y - 1u < ny - 2u) && (z - 1u < nz - 2u));
     if (PARITY == 0) {
 #pragma unroll
-        for (int q = 0; q < 19; q++) d[q] = IO::ld(P + q * S + i, isc);
+        for (int q = 0; q < 19; q++) d[q] = IO::ld(P + (q * S + i), isc);
     } else if (fast) {
 #pragma unroll
         for (int q = 0; q < 19; q++) {
@@ -307,11 +332,11 @@ __global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
             const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
             const unsigned nbr = i - (unsigned)(cx + cy * (int)nx + cz * (int)nxy);
             if (cx == 0) {
-                d[q] = IO::ld(P + qopp(q) * S + nbr, isc);
+                d[q] = IO::ld(P + (qopp(q) * S + nbr), isc);
             } else {
                 const bool edge = (cx > 0) ? (x == 0) : (x == nx - 1);
                 if (PERX)
-                    d[q] = IO::ld(P + qopp(q) * S + (edge ? nbr + (unsigned)(cx * (int)nx) : nbr), isc);
+                    d[q] = IO::ld(P + (qopp(q) * S + (edge ? nbr + (unsigned)(cx * (int)nx) : nbr)), isc);
                 else
                     d[q] = IO::ld(P + (edge ? q * S + i : qopp(q) * S + nbr), isc);
             }
@@ -356,11 +381,14 @@ __global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
     }
     float ux, uy, uz, rho;
     collide(d, Fx, Fy, Fz, F.omega, F.fpref, ux, uy, uz, rho);
+    // recompute store addresses from an opaque copy of the base pointer instead
+    // of keeping the 19 load addresses alive across the collision
+    asm volatile("mov.b64 %0, %0;" : "+l"(P));
 
     const float sc = F.scale;
     if (PARITY == 0) {
 #pragma unroll
-        for (int q = 0; q < 19; q++) IO::st(P + qopp(q) * S + i, d[q], sc);
+        for (int q = 0; q < 19; q++) IO::st(P + (qopp(q) * S + i), d[q], sc);
     } else if (fast) {
 #pragma unroll
         for (int q = 0; q < 19; q++) {
@@ -369,11 +397,11 @@ __global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
             const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
             const unsigned nbr = i + (unsigned)(cx + cy * (int)nx + cz * (int)nxy);
             if (cx == 0) {
-                IO::st(P + q * S + nbr, d[q], sc);
+                IO::st(P + (q * S + nbr), d[q], sc);
             } else {
                 const bool edge = (cx > 0) ? (x == nx - 1) : (x == 0);
                 if (PERX)
-                    IO::st(P + q * S + (edge ? nbr - (unsigned)(cx * (int)nx) : nbr), d[q], sc);
+                    IO::st(P + (q * S + (edge ? nbr - (unsigned)(cx * (int)nx) : nbr)), d[q], sc);
                 else
                     IO::st(P + (edge ? qopp(q) * S + i : q * S + nbr), d[q], sc);
             }
@@ -409,6 +437,102 @@ __global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
     if (inb || a.last) F.u[i] = make_float4(ux, uy, uz, rho);
 }
 
+// Per-tile state prepared by warp 0 one tile ahead: the ticket and the marker
+// boxes that overlap the tile's cells.
+struct TileSlot {
+    unsigned t;
+    int nb;
+    Box b[kMaxBoxes];
+};
+
+__device__ __forceinline__ void prepare_slot(const StepArgs& a, unsigned t, TileSlot& sl) {
+    const unsigned lane = threadIdx.x & 31;
+    int nb = 0;
+    if (t >= (unsigned)a.n_ibm && t < (unsigned)(a.n_ibm + a.n_tiles)) {
+        const FluidDev& F = a.F;
+        const unsigned c0 = (t - a.n_ibm) * kTileCells;
+        const unsigned c1 = min(c0 + kTileCells - 1, (unsigned)F.N - 1);
+        const TileExt ext = tile_extent(c0, c1, F.nx, F.ny, a.div_nx, a.div_nxy);
+        for (int j0 = 0; j0 < a.n_boxes; j0 += 32) {
+            const int j = j0 + (int)lane;
+            Box b{1, 0, 1, 0, 1, 0};
+            bool hit = false;
+            if (j < a.n_boxes) {
+                b = a.Mk.boxes[j];
+                hit = b.x0 <= b.x1 && overlaps(b, ext);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (hit) sl.b[nb + __popc(m & ((1u << lane) - 1u))] = b;
+            nb += __popc(m);
+        }
+    }
+    if (lane == 0) {
+        sl.t = t;
+        sl.nb = nb;
+    }
+}
+
+// a lattice tile of kTileCells consecutive cells, kCellsPerThread per thread
+template <int ST, int PARITY, int PERX>
+__device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const TileSlot& sl) {
+    const FluidDev& F = a.F;
+    const unsigned c0 = tile * kTileCells;
+    const unsigned c1 = min(c0 + kTileCells - 1, (unsigned)F.N - 1);
+    const int nb = sl.nb;
+    if (nb > 0) wait_ibm(a);
+#pragma unroll 1
+    for (int r = 0; r < kCellsPerThread; r++) {
+        const unsigned i = c0 + r * kTile + threadIdx.x;
+        if (i <= c1) {
+            bool inb = false;
+            if (nb > 0) {
+                const unsigned z = fdiv(i, a.div_nxy);
+                const unsigned rem = i - z * (F.nx * F.ny);
+                const unsigned y = fdiv(rem, a.div_nx);
+                const unsigned x = rem - y * F.nx;
+                for (int j = 0; j < nb; j++) inb |= inside(sl.b[j], (int)x, (int)y, (int)z);
+            }
+            lbm_cell<ST, PARITY, PERX>(a, i, inb);
+        }
+    }
+}
+
+// Persistent substep kernel: each CTA takes tickets until none are left.
+// Tickets [0, n_ibm) are IBM tasks, the rest lattice tiles in cell order.  A
+// tile that meets a marker box waits for all IBM tasks of this substep; every
+// IBM ticket is held by a CTA that runs it before taking another ticket, so
+// the wait always ends (it is also bounded).  Warp 0 fetches the next ticket
+// and prepares its tile while the CTA works on the current one, so each tile
+// costs one block barrier.
+template <int ST, int PARITY, int PERX>
+__global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
+    __shared__ TileSlot s_slot[2];
+    const unsigned total = (unsigned)a.n_ibm + (unsigned)a.n_tiles;
+    const bool warp0 = threadIdx.x < 32;
+    if (warp0) {
+        unsigned t0 = 0;
+        if (threadIdx.x == 0) t0 = atomicAdd(&a.tickets[a.k], 1u);
+        t0 = __shfl_sync(0xffffffffu, t0, 0);
+        prepare_slot(a, t0, s_slot[0]);
+    }
+    __syncthreads();
+    for (int j = 0;; j ^= 1) {
+        const unsigned t = s_slot[j].t;
+        if (t >= total) break;
+        unsigned tn = 0;
+        if (threadIdx.x == 0) tn = atomicAdd(&a.tickets[a.k], 1u);
+        if (t < (unsigned)a.n_ibm)
+            ibm_task(a, t);
+        else
+            lbm_tile<ST, PARITY, PERX>(a, t - a.n_ibm, s_slot[j]);
+        if (warp0) {
+            tn = __shfl_sync(0xffffffffu, tn, 0);
+            prepare_slot(a, tn, s_slot[j ^ 1]);
+        }
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------------------
 // upwind advection + diffusion of the concentration (once per iteration)
 // ---------------------------------------------------------------------------
@@ -425,7 +549,7 @@ __global__ void __launch_bounds__(kTile) conv_diff_kernel(ConcArgs a) {
     const unsigned N = (unsigned)F.N, nxy = nx * ny;
     const unsigned c0 = blockIdx.x * kTile;
     const unsigned c1 = min(c0 + kTile - 1, N - 1);
-    const TileExt ext = tile_extent(c0, c1, nx, ny);
+    const TileExt ext = tile_extent(c0, c1, nx, ny, a.div_nx, a.div_nxy);
     const int nb = tile_boxes(a.Mk.boxes, a.n_boxes, ext, s_b, &s_nb);
     const unsigned i = c0 + threadIdx.x;
     if (i > c1) return;
@@ -517,7 +641,16 @@ __global__ void write_pop_kernel(FluidDev F, const float* in) {
 // host-side launchers
 // ---------------------------------------------------------------------------
 int lbm_grid(const StepArgs& a) {
-    return a.n_ibm + (int)((a.F.N + kTile - 1) / kTile);
+    const int total = a.n_ibm + a.n_tiles;
+    return a.lbm_ctas > 0 ? min(total, a.lbm_ctas) : total;
+}
+
+int lbm_resident_ctas() {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF32, 1, 0>, kTile, 0);
+    return max(1, sms * max(1, per_sm));
 }
 
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {

@@ -17,6 +17,8 @@ struct StepArgs {
     int k;               // substep index within the iteration
     int last;            // k == nsub - 1: write u for every cell
     FastDiv div_nx, div_nxy;
+    int n_tiles;         // lattice tiles of kTile cells
+    int lbm_ctas;        // persistent CTAs per launch (0: one per ticket)
 };
 
 struct ConcArgs {
@@ -30,6 +32,7 @@ struct ConcArgs {
 };
 
 int lbm_grid(const StepArgs& a);
+int lbm_resident_ctas();
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s);
 cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s);
 cudaError_t launch_read_pop(const FluidDev& F, int natural, float* out, cudaStream_t s);
