@@ -200,6 +200,40 @@ int glsm_fluid_profile_velocity(glsm_fluid f, int iter, float* ms);
 /* gel_to_lbm_vel and lbm_to_gel_vel (src/fluid.cu:221-222) */
 int glsm_fluid_units(glsm_fluid f, float out[2]);
 
+/* ---- Substep without device allocation ------------------------------------
+ * No counterpart in the reference: an extra entry point for callers that cannot
+ * call cudaMalloc (a host framework that owns all device memory through its own
+ * pool, a plug-in whose host process must account for every device byte, a
+ * real-time loop where an allocation may synchronise the device).  Such callers
+ * cannot create the handles above, which own their buffers.
+ *
+ * One LBM substep with immersed-boundary forcing on caller-owned device
+ * buffers, enqueued on `stream` (a cudaStream_t, NULL for the default stream):
+ *   pop      19 planes of `plane_stride` floats: population deviations f_q - w_q
+ *            in the D3Q19 order of the reference, updated in place with the AA
+ *            pattern (parity 0 turns natural-layout post-stream values into
+ *            post-collision values in reversed slots; parity 1 turns those back
+ *            into natural post-stream values, so two calls make one full step)
+ *   u4       per cell (ux, uy, uz, rho): read as the previous substep's velocity
+ *            for the interpolation, overwritten with this substep's
+ *   lag4     per marker (x, y, z, -) positions in physical units (lattice
+ *            coordinate = position / h); vel4 per marker target velocity (lattice)
+ *   Ul4, Fdrag4  per marker outputs: interpolated velocity, penalty force
+ * Walls bounce back on all six faces; tau, the uniform force (fx, fy, fz) and
+ * beta_eff are the BGK relaxation time, F_const and the ramped IBM penalty.
+ * Limits: at most 262,144 lattice cells and 16,384 markers per call.  The
+ * scratch lives in one file-scope device array of 5,308,416 bytes that every
+ * GPU loading the library holds until the process exits; the first call on a
+ * device looks up its address, so make that first call before any stream
+ * capture.  All calls on a device share the scratch (it is cleared at the
+ * start of each call): calls that overlap on the GPU race on it.
+ * Returns GLSM_OK or a negative status; glsm_noalloc_last_error() explains. */
+int glsm_substep_noalloc(float* pop, int64_t plane_stride, float* u4, int nx, int ny, int nz, int parity, float tau,
+                         float fx, float fy, float fz, const float* lag4, const float* vel4, int n_markers, float h,
+                         float beta_eff, float* Ul4, float* Fdrag4, void* stream);
+const char* glsm_noalloc_last_error(void);
+size_t glsm_noalloc_scratch_bytes(void);
+
 #ifdef __cplusplus
 }
 #endif
