@@ -38,7 +38,7 @@ FLUSH_BYTES = 256 << 20  # > the 126 MB L2
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
@@ -80,9 +80,9 @@ def ncu_traffic(storage):
 
 
 class Clocks:
-    """nvidia-smi samples during the timed region."""
+    """nvidia-smi samples; stats are taken over the samples inside [t0, t1]."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -94,14 +94,17 @@ class Clocks:
     def start(self):
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-i", str(self.index), "-lms", "200"], stdout=self.f,
+                                       "-i", str(self.index), "-lms", "100"], stdout=self.f,
                                       stderr=subprocess.DEVNULL)
         except OSError:
             self.p = None
 
-    def stop(self):
+    def stop(self, t0, t1):
+        import datetime
+
         if self.p is None:
             return None
+        time.sleep(0.25)
         self.p.terminate()
         try:
             self.p.wait(timeout=5)
@@ -109,26 +112,28 @@ class Clocks:
             self.p.kill()
         self.f.flush()
         self.f.seek(0)
-        sm, mx, reasons = [], [], set()
+        rows = []
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for line in self.f.read().splitlines():
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1]))
-                mx.append(float(parts[2]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(parts[2]), float(parts[3]), float(parts[4]),
+                             {n for n, v in zip(names, parts[6:10]) if v.lower().startswith("active")}))
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
         os.unlink(self.f.name)
-        if not sm:
+        if not rows:
             return None
-        loaded = [s for s in sm if s > 0.5 * max(sm)] or sm
-        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        inside = [r for r in rows if t0 - 0.05 <= r[0] <= t1 + 0.05]
+        if not inside:  # region shorter than the sampling interval: the samples around it
+            inside = sorted(rows, key=lambda r: min(abs(r[0] - t0), abs(r[0] - t1)))[:2]
+        sm = [r[1] for r in inside]
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(r[2] for r in inside),
+                "power_w_max": max(r[3] for r in inside),
+                "reasons": sorted(set().union(*[r[4] for r in inside])), "samples": len(inside)}
 
 
 def dist_setup(args):
@@ -190,11 +195,14 @@ def run_ours(args, world, rank, local):
     fluid = s.fluid
     stream = torch.cuda.ExternalStream(s.coupler.stream())
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    clocks = Clocks(local)
+    clocks.start()
     it = 0
     for _ in range(args.warmup):
         fluid.run(it, 1)
         it += 1
     fluid.sync()
+    time.sleep(0.3)  # let the sampler settle
 
     def barrier():
         if world > 1:
@@ -203,9 +211,8 @@ def run_ours(args, world, rank, local):
 
     K = args.steps
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-    clocks = Clocks(local)
     barrier()
-    clocks.start()
+    t_wall0 = time.time()
     for k in range(K):
         with torch.cuda.stream(stream):
             flush.zero_()
@@ -215,7 +222,8 @@ def run_ours(args, world, rank, local):
         it += 1
     stream.synchronize()
     barrier()
-    clk = clocks.stop()
+    t_wall1 = time.time()
+    clk = clocks.stop(t_wall0, t_wall1)
     fluid.sync()
     t_ms = sum(a.elapsed_time(b) for a, b in ev)
     if world > 1:
@@ -338,17 +346,19 @@ def run_reference(args, world, rank, local):
     it = 0
     r.time(it, args.warmup)
     it += args.warmup
-    K = args.steps
+    K = min(args.steps, 300)  # the reference is ~8 ms per step
     clocks = Clocks(local)
-    torch.cuda.synchronize()
     clocks.start()
+    time.sleep(0.3)
+    torch.cuda.synchronize()
+    t_wall0 = time.time()
     t_ms = 0.0
     for _ in range(K):
         flush.zero_()  # legacy default stream: ordered with the reference's streams
         t_ms += r.time(it, 1)
         it += 1
     torch.cuda.synchronize()
-    clk = clocks.stop()
+    clk = clocks.stop(t_wall0, time.time())
     r.close()
     N = DIMS[0] * DIMS[1] * DIMS[2]
     value = N * NSUB * K / (t_ms / 1e3) / 1e6
