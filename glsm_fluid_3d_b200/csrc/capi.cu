@@ -56,6 +56,7 @@ struct glsm_gel_s {
     double* series_extra = nullptr;  // a time-series ring larger than the built-in one
     glsm_coupler_s* coupler = nullptr;
     int index = -1;             // position in the coupler
+    bool release_with_coupler = false;  // destroyed while coupled: freed with the coupler
 };
 
 struct glsm_coupler_s {
@@ -288,7 +289,8 @@ int glsm_gel_create(int sx, int sy, int sz, double px, double py, double pz, int
                 if (x == 1 || x == d.LX || y == 1 || y == d.LY || z == 1 || z == d.LZ)
                     surf.push_back(x + (d.LX + 2) * (y + (d.LY + 2) * z));
 
-    e = cudaStreamCreateWithFlags(&g->own, cudaStreamNonBlocking);
+    // blocking streams, like the reference's: legacy-stream copies order after queued work
+    e = cudaStreamCreate(&g->own);
     if (e == cudaSuccess) e = cudaMemset(g->arena, 0, bytes);
     if (e == cudaSuccess) e = cudaMemcpy(d.um, um.data(), nE * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(d.vm, vm.data(), nE * sizeof(double), cudaMemcpyHostToDevice);
@@ -306,14 +308,23 @@ int glsm_gel_create(int sx, int sy, int sz, double px, double py, double pz, int
     return GLSM_OK;
 }
 
-int glsm_gel_destroy(glsm_gel g) {
-    if (!g) return GLSM_OK;
-    if (g->coupler) return fail(GLSM_ERR_STATE, "destroy the coupler before its gels");
+static void gel_release(glsm_gel g) {
     cudaStreamSynchronize(g->own);
     cudaStreamDestroy(g->own);
     if (g->series_extra) cudaFree(g->series_extra);
     cudaFree(g->arena);
     delete g;
+}
+
+int glsm_gel_destroy(glsm_gel g) {
+    if (!g) return GLSM_OK;
+    if (g->coupler) {
+        // the reference's drivers delete their gels before the fluid and the
+        // coupler (src/sim.cpp:143-146): the gel is released with its coupler
+        g->release_with_coupler = true;
+        return GLSM_OK;
+    }
+    gel_release(g);
     return GLSM_OK;
 }
 
@@ -592,8 +603,8 @@ int glsm_coupler_create(const glsm_gel* gels, int n_gels, glsm_coupler* out) {
         off += g->d.M;
         c->gels.push_back(g);
     }
-    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking);
+    e = cudaStreamCreate(&c->stream);
+    if (e == cudaSuccess) e = cudaStreamCreate(&c->side);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&c->h_ctl, sizeof(Ctl), cudaHostAllocDefault);
@@ -628,6 +639,7 @@ int glsm_coupler_destroy(glsm_coupler c) {
     for (auto* g : c->gels) {
         g->coupler = nullptr;
         g->index = -1;
+        if (g->release_with_coupler) gel_release(g);
     }
     cudaEventDestroy(c->ev_fork);
     cudaEventDestroy(c->ev_join);

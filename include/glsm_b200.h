@@ -114,7 +114,8 @@ int glsm_version(void);
  * gel.cu:424-450; node lattice, gel.cu:179-219; surface order, gel.cu:161-177) */
 int glsm_gel_create(int sx, int sy, int sz, double px, double py, double pz, int gel_type, int gel_id,
                     glsm_gel* out);
-/* Gel::~Gel, src/gel.cu:665-668 */
+/* Gel::~Gel, src/gel.cu:665-668.  A gel that still belongs to a coupler is
+ * released together with that coupler (it must not be used in between). */
 int glsm_gel_destroy(glsm_gel g);
 /* sizes: LX, LY, LZ, element slots, node slots, markers, gel id, gel type */
 int glsm_gel_info(glsm_gel g, int64_t out[8]);
