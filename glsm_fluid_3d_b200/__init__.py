@@ -26,7 +26,7 @@ import numpy as np
 
 from ._lib import FluidDesc, GlsmError, check, lib
 
-__all__ = ["Gel", "Coupler", "Fluid", "System", "GlsmError", "STORAGE", "lib"]
+__all__ = ["Gel", "Coupler", "Fluid", "System", "Batch", "GlsmError", "STORAGE", "lib"]
 
 STORAGE = {"f32": 0, "fp32": 0, "f16": 1, "fp16": 1, "bf16": 2}
 
@@ -99,6 +99,10 @@ class Gel:
     # extensions ---------------------------------------------------------------
     def set_active_from(self, it):
         check(self.L.glsm_gel_set_active_from(self.h, int(it)), "set_active_from")
+
+    def set_bz_f(self, f):
+        """GelParams::f; recomputes the steady state and restarts the chemistry from it."""
+        check(self.L.glsm_gel_set_bz_f(self.h, float(f)), "set_bz_f")
 
     def add_noise(self, seed, amplitude):
         check(self.L.glsm_gel_add_noise(self.h, int(seed), float(amplitude)), "add_noise")
@@ -278,6 +282,40 @@ class Fluid:
             check(self.L.glsm_fluid_destroy(self.h), "Fluid destroy")
             self.h = None
             self.coupler.fluid = None
+
+
+class Batch:
+    """Several systems advanced together by batched launches (include/glsm_b200.h glsm_batch_*)."""
+
+    def __init__(self):
+        self.L = lib()
+        h = ctypes.c_void_p()
+        check(self.L.glsm_batch_create(ctypes.byref(h)), "Batch")
+        self.h = h
+        self.members = []
+
+    def add(self, fluid, iter0=0):
+        check(self.L.glsm_batch_add(self.h, fluid.h, int(iter0)), "batch add")
+        self.members.append(fluid)
+
+    def remove(self, fluid):
+        check(self.L.glsm_batch_remove(self.h, fluid.h), "batch remove")
+        self.members.remove(fluid)
+
+    def run(self, n):
+        check(self.L.glsm_batch_run(self.h, int(n)), "batch run")
+
+    def sync(self):
+        check(self.L.glsm_batch_sync(self.h), "batch sync")
+
+    def __len__(self):
+        return self.L.glsm_batch_size(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            check(self.L.glsm_batch_destroy(self.h), "Batch destroy")
+            self.h = None
+            self.members = []
 
 
 class System:

@@ -70,6 +70,14 @@ def lib():
         "glsm_fluid_info": [vp, P(ctypes.c_int64)],
         "glsm_fluid_units": [vp, P(f)],
         "glsm_fluid_profile_velocity": [vp, i, P(f)],
+        "glsm_gel_set_bz_f": [vp, d],
+        "glsm_batch_create": [P(vp)],
+        "glsm_batch_destroy": [vp],
+        "glsm_batch_add": [vp, vp, i],
+        "glsm_batch_remove": [vp, vp],
+        "glsm_batch_size": [vp],
+        "glsm_batch_run": [vp, i],
+        "glsm_batch_sync": [vp],
     }
     for name, args in sig.items():
         fn = getattr(L, name)

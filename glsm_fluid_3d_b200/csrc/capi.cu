@@ -84,6 +84,7 @@ struct glsm_fluid_s {
     long long substeps = 0;      // AA parity bookkeeping
     float* scratch = nullptr;    // 19*N floats, allocated on first use
     int lbm_ctas = 0;            // resident CTAs of the persistent substep kernel
+    struct glsm_batch_s* batch = nullptr;  // batch this system belongs to
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 };
 
@@ -519,6 +520,24 @@ int glsm_gel_build_tube_mask(glsm_gel g, int wall_thickness, int circular) {
     });
 }
 
+int glsm_gel_set_bz_f(glsm_gel g, double f) {
+    if (!g || !(f > 0.0)) return fail(GLSM_ERR_ARG, "f must be positive");
+    GelDev& d = g->d;
+    d.f = f;
+    bz_steady_state(d.f, 1e-4, d.FA0, d.uss, d.vss, d.wss);
+    int r = upload_gel_desc(g);
+    if (r) return r;
+    // the interior starts at the new steady state (src/gel.cu:184-200)
+    const GelDev dd = d;
+    return edit_chemistry(g, [&](int x, int y, int z, double& u, double& v, double& w) {
+        if (x >= 1 && x < dd.LX && y >= 1 && y < dd.LY && z >= 1 && z < dd.LZ) {
+            u = dd.uss;
+            v = dd.vss;
+            w = dd.wss;
+        }
+    });
+}
+
 int glsm_gel_set_active_from(glsm_gel g, int iter) {
     if (!g || iter < 0) return fail(GLSM_ERR_ARG, "iteration must be >= 0");
     g->d.active_from = iter;
@@ -862,6 +881,7 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
 
 int glsm_fluid_destroy(glsm_fluid f) {
     if (!f) return GLSM_OK;
+    if (f->batch) return fail(GLSM_ERR_STATE, "remove the system from its batch first");
     cudaStreamSynchronize(f->c->stream);
     for (auto& row : f->graph)
         for (auto& g : row)
@@ -904,6 +924,7 @@ static int enqueue_velocity(glsm_fluid f, int iter_arg, cudaStream_t s) {
 
 int glsm_fluid_step_velocity(glsm_fluid f, int iter) {
     if (!f || iter < 0) return fail(GLSM_ERR_ARG, "bad argument");
+    if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
     int r = enqueue_velocity(f, iter, f->c->stream);
     if (r) return r;
     f->substeps += f->F.nsub;
@@ -912,6 +933,7 @@ int glsm_fluid_step_velocity(glsm_fluid f, int iter) {
 
 int glsm_fluid_step_concentration(glsm_fluid f, int iter) {
     if (!f || iter < 0) return fail(GLSM_ERR_ARG, "bad argument");
+    if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
     glsm_coupler c = f->c;
     MarkerArgs m{c->d_gels, c->mk, f->F.c[f->cur], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 0};
     CK(launch_conc_markers(m, c->stream));
@@ -973,6 +995,7 @@ static int get_graph(glsm_fluid f, int p0, int cur, cudaGraphExec_t* out) {
 
 int glsm_fluid_run(glsm_fluid f, int iter0, int n) {
     if (!f || iter0 < 0 || n < 0) return fail(GLSM_ERR_ARG, "bad argument");
+    if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
     if (n == 0) return GLSM_OK;
     glsm_coupler c = f->c;
     set_iter_kernel<<<1, 1, 0, c->stream>>>(c->d_ctl, iter0);
@@ -1069,8 +1092,11 @@ __global__ void u_unpack_kernel(const float* in, long long N, float4* u) {
     u[i] = make_float4(in[3 * i], in[3 * i + 1], in[3 * i + 2], 1.0f);
 }
 
+static int batch_wait(glsm_fluid f);
+
 int glsm_fluid_read(glsm_fluid f, int field, float* dst, size_t count) {
     if (!f || !dst) return fail(GLSM_ERR_ARG, "null argument");
+    if (int r = batch_wait(f)) return r;
     cudaStream_t s = f->c->stream;
     const long long N = f->F.N;
     const unsigned blocks = (unsigned)((N + 255) / 256);
@@ -1113,6 +1139,7 @@ int glsm_fluid_read(glsm_fluid f, int field, float* dst, size_t count) {
 
 int glsm_fluid_write(glsm_fluid f, int field, const float* src, size_t count) {
     if (!f || !src) return fail(GLSM_ERR_ARG, "null argument");
+    if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
     cudaStream_t s = f->c->stream;
     const long long N = f->F.N;
     const unsigned blocks = (unsigned)((N + 255) / 256);
@@ -1139,6 +1166,241 @@ int glsm_fluid_write(glsm_fluid f, int field, const float* src, size_t count) {
         default: return fail(GLSM_ERR_ARG, "field %d is not writable", field);
     }
     CK(cudaStreamSynchronize(s));
+    return GLSM_OK;
+}
+
+
+// ===========================================================================
+// Batch: several systems advanced together
+// ===========================================================================
+struct glsm_batch_s {
+    std::vector<glsm_fluid_s*> sys;
+    int nsub = 0;
+    cudaStream_t stream = nullptr, side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    void* arena = nullptr;
+    BatchSys* d_sys = nullptr;
+    SysDyn* d_dyn = nullptr;
+    GelArgs* d_gel = nullptr;
+    MarkerArgs* d_mark = nullptr;
+    RepulsionArgs* d_rep = nullptr;
+    int *d_ibm_off = nullptr, *d_tile_off = nullptr, *d_conv_off = nullptr, *d_warp_off = nullptr,
+        *d_rep_off = nullptr;
+    unsigned *d_tickets = nullptr, *d_ibm_done = nullptr;
+    int n_gels = 0, warps = 0, rep_blocks = 0, conv_blocks = 0;
+    int resident = 0;
+    bool dirty = true;
+    cudaGraphExec_t graph = nullptr;
+};
+
+static int batch_wait(glsm_fluid f) {
+    if (f->batch) CK(cudaStreamSynchronize(f->batch->stream));
+    return GLSM_OK;
+}
+
+static void batch_free_device(glsm_batch_s* b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    if (b->arena) cudaFree(b->arena);
+    b->arena = nullptr;
+}
+
+// device descriptors of the current members; recapture of the iteration graph
+static int batch_rebuild(glsm_batch_s* b) {
+    CK(cudaStreamSynchronize(b->stream));
+    batch_free_device(b);
+    const int n = (int)b->sys.size();
+    b->dirty = false;
+    if (n == 0) return GLSM_OK;
+    std::vector<BatchSys> hs(n);
+    std::vector<SysDyn> hd(n);
+    std::vector<GelArgs> hg;
+    std::vector<MarkerArgs> hm(2 * (size_t)n);
+    std::vector<RepulsionArgs> hr(n);
+    std::vector<int> ibm_off(n + 1, 0), tile_off(n + 1, 0), conv_off(n + 1, 0), warp_off(n + 1, 0), rep_off(n + 1, 0);
+    for (int i = 0; i < n; i++) {
+        glsm_fluid_s* f = b->sys[i];
+        glsm_coupler c = f->c;
+        StepArgs a = step_args(f, 0, -1);
+        hs[i].step = a;
+        hs[i].conc = ConcArgs{f->F, c->mk, c->d_ctl, (int)c->gels.size(), 0, 0, make_fastdiv((unsigned)f->F.nx),
+                              make_fastdiv((unsigned)(f->F.nx * f->F.ny))};
+        hd[i].parity0 = (int)(f->substeps & 1);
+        hd[i].cur = f->cur;
+        for (int cb = 0; cb < 2; cb++)
+            hm[2 * i + cb] = MarkerArgs{c->d_gels, c->mk, f->F.c[cb], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 1};
+        hr[i] = RepulsionArgs{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 1};
+        const int phases = kPhElastic | kPhChem | kPhRecord | kPhGather | kPhAuto;
+        for (int g = 0; g < (int)c->gels.size(); g++) {
+            GelArgs ga = coupler_gel_args(c, phases, -1);
+            ga.first_gel = g;
+            hg.push_back(ga);
+        }
+        ibm_off[i + 1] = ibm_off[i] + a.n_ibm;
+        tile_off[i + 1] = tile_off[i] + a.n_tiles;
+        conv_off[i + 1] = conv_off[i] + (int)((f->F.N + kTile - 1) / kTile);
+        warp_off[i + 1] = warp_off[i] + c->mk.M;
+        rep_off[i + 1] = rep_off[i] + (c->mk.M + 255) / 256;
+    }
+    b->n_gels = (int)hg.size();
+    b->warps = warp_off[n];
+    b->rep_blocks = rep_off[n];
+    b->conv_blocks = conv_off[n];
+    size_t bytes;
+    {
+        Carver cv{nullptr};
+        cv.take<BatchSys>(n);
+        cv.take<SysDyn>(n);
+        cv.take<GelArgs>(std::max<size_t>(1, hg.size()));
+        cv.take<MarkerArgs>(2 * (size_t)n);
+        cv.take<RepulsionArgs>(n);
+        for (int k = 0; k < 5; k++) cv.take<int>(n + 1);
+        cv.take<unsigned>(b->nsub);
+        cv.take<unsigned>((size_t)n * b->nsub);
+        bytes = align_up(cv.off, 256);
+    }
+    CK(cudaMalloc(&b->arena, bytes));
+    Carver cv{(char*)b->arena};
+    b->d_sys = cv.take<BatchSys>(n);
+    b->d_dyn = cv.take<SysDyn>(n);
+    b->d_gel = cv.take<GelArgs>(std::max<size_t>(1, hg.size()));
+    b->d_mark = cv.take<MarkerArgs>(2 * (size_t)n);
+    b->d_rep = cv.take<RepulsionArgs>(n);
+    b->d_ibm_off = cv.take<int>(n + 1);
+    b->d_tile_off = cv.take<int>(n + 1);
+    b->d_conv_off = cv.take<int>(n + 1);
+    b->d_warp_off = cv.take<int>(n + 1);
+    b->d_rep_off = cv.take<int>(n + 1);
+    b->d_tickets = cv.take<unsigned>(b->nsub);
+    b->d_ibm_done = cv.take<unsigned>((size_t)n * b->nsub);
+    for (int i = 0; i < n; i++) {
+        hs[i].dyn = b->d_dyn + i;
+        hs[i].step.ibm_done = b->d_ibm_done + (size_t)i * b->nsub;
+        hs[i].step.tickets = b->d_tickets;
+    }
+    CK(cudaMemcpy(b->d_sys, hs.data(), n * sizeof(BatchSys), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_dyn, hd.data(), n * sizeof(SysDyn), cudaMemcpyHostToDevice));
+    if (!hg.empty()) CK(cudaMemcpy(b->d_gel, hg.data(), hg.size() * sizeof(GelArgs), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_mark, hm.data(), hm.size() * sizeof(MarkerArgs), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_rep, hr.data(), hr.size() * sizeof(RepulsionArgs), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_ibm_off, ibm_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_tile_off, tile_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_conv_off, conv_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_warp_off, warp_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_rep_off, rep_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+
+    // capture one batch iteration
+    cudaStream_t st = b->stream;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaMemsetAsync(b->d_tickets, 0, b->nsub * sizeof(unsigned), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ibm_done, 0, (size_t)n * b->nsub * sizeof(unsigned), st);
+    if (e == cudaSuccess) e = launch_gel_batch(b->d_gel, b->n_gels, b->n_gels, st);
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev_fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->ev_fork, 0);
+    if (e == cudaSuccess) e = launch_conc_markers_batch(b->d_mark, b->d_dyn, b->d_warp_off, n, b->warps, b->side);
+    if (e == cudaSuccess) e = launch_repulsion_batch(b->d_rep, b->d_rep_off, n, b->rep_blocks, b->side);
+    if (e == cudaSuccess) e = cudaEventRecord(b->ev_join, b->side);
+    for (int k = 0; k < b->nsub && e == cudaSuccess; k++) {
+        BatchLaunch L{b->d_sys, b->d_ibm_off, b->d_tile_off, b->d_tickets, n, k, k == b->nsub - 1};
+        e = launch_substep_batch(L, std::min(b->resident, ibm_off[n] + tile_off[n]), st);
+    }
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->ev_join, 0);
+    if (e == cudaSuccess) e = launch_conv_diff_batch(b->d_sys, b->d_conv_off, n, b->conv_blocks, st);
+    if (e == cudaSuccess) e = launch_batch_advance(b->d_sys, n, st);
+    cudaError_t e2 = cudaStreamEndCapture(st, &g);
+    if (e != cudaSuccess || e2 != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(GLSM_ERR_CUDA, "batch capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(GLSM_ERR_CUDA, "batch instantiate: %s", cudaGetErrorString(e));
+    return GLSM_OK;
+}
+
+int glsm_batch_create(glsm_batch* out) {
+    if (!out) return fail(GLSM_ERR_ARG, "null argument");
+    auto* b = new glsm_batch_s;
+    cudaError_t e = cudaStreamCreate(&b->stream);
+    if (e == cudaSuccess) e = cudaStreamCreate(&b->side);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        delete b;
+        return fail(GLSM_ERR_CUDA, "batch: %s", cudaGetErrorString(e));
+    }
+    b->resident = batch_resident_ctas();
+    *out = b;
+    return GLSM_OK;
+}
+
+int glsm_batch_add(glsm_batch b, glsm_fluid f, int iter0) {
+    if (!b || !f || iter0 < 0) return fail(GLSM_ERR_ARG, "bad argument");
+    if (f->batch) return fail(GLSM_ERR_STATE, "system already in a batch");
+    if (!b->sys.empty() && f->F.nsub != b->nsub) return fail(GLSM_ERR_ARG, "all systems of a batch need the same nsub");
+    CK(cudaStreamSynchronize(f->c->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    if (b->sys.empty()) b->nsub = f->F.nsub;
+    set_iter_kernel<<<1, 1, 0, b->stream>>>(f->c->d_ctl, iter0);
+    CK(cudaGetLastError());
+    f->batch = b;
+    b->sys.push_back(f);
+    b->dirty = true;
+    return GLSM_OK;
+}
+
+int glsm_batch_remove(glsm_batch b, glsm_fluid f) {
+    if (!b || !f || f->batch != b) return fail(GLSM_ERR_ARG, "system is not in this batch");
+    CK(cudaStreamSynchronize(b->stream));
+    b->sys.erase(std::find(b->sys.begin(), b->sys.end(), f));
+    f->batch = nullptr;
+    b->dirty = true;
+    return GLSM_OK;
+}
+
+int glsm_batch_size(glsm_batch b) { return b ? (int)b->sys.size() : 0; }
+
+int glsm_batch_run(glsm_batch b, int n) {
+    if (!b || n < 0) return fail(GLSM_ERR_ARG, "bad argument");
+    if (b->dirty) {
+        int r = batch_rebuild(b);
+        if (r) return r;
+    }
+    if (b->sys.empty() || n == 0) return GLSM_OK;
+    for (int it = 0; it < n; it++) CK(cudaGraphLaunch(b->graph, b->stream));
+    for (auto* f : b->sys) {
+        f->substeps += (long long)n * f->F.nsub;
+        f->cur ^= (n & 1);
+    }
+    return GLSM_OK;
+}
+
+int glsm_batch_sync(glsm_batch b) {
+    if (!b) return fail(GLSM_ERR_ARG, "null batch");
+    CK(cudaStreamSynchronize(b->stream));
+    for (auto* f : b->sys) {
+        glsm_coupler c = f->c;
+        CK(cudaMemcpy(c->h_ctl, c->d_ctl, sizeof(Ctl), cudaMemcpyDeviceToHost));
+        if (c->h_ctl->error) {
+            const int err = c->h_ctl->error;
+            CK(cudaMemset(&c->d_ctl->error, 0, sizeof(int)));
+            return fail(GLSM_ERR_DEVICE, "device error flags 0x%x in a batch member", err);
+        }
+    }
+    return GLSM_OK;
+}
+
+int glsm_batch_destroy(glsm_batch b) {
+    if (!b) return GLSM_OK;
+    cudaStreamSynchronize(b->stream);
+    for (auto* f : b->sys) f->batch = nullptr;
+    batch_free_device(b);
+    cudaEventDestroy(b->ev_fork);
+    cudaEventDestroy(b->ev_join);
+    cudaStreamDestroy(b->side);
+    cudaStreamDestroy(b->stream);
+    delete b;
     return GLSM_OK;
 }
 

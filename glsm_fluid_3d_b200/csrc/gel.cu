@@ -359,7 +359,7 @@ __device__ void record_center(const GelDev& G, const Idx& I, int iter) {
 }
 
 // k_gather_boundary + the per-iteration stencil cache and the force-region box
-__device__ void gather(const GelDev& G, const GelArgs& a, int* s_box) {
+__device__ void gather(const GelDev& G, const GelArgs& a, int gel_index, int* s_box) {
     const MarkerDev& Mk = a.Mk;
     if (threadIdx.x < 6) s_box[threadIdx.x] = (threadIdx.x & 1) ? -1 : 0x7fffffff;
     __syncthreads();
@@ -421,13 +421,13 @@ _Pragma("unroll")
         b.z0 = s_box[4];
         b.z1 = s_box[5];
         if (b.x1 < 0 || b.y1 < 0 || b.z1 < 0) b = Box{1, 0, 1, 0, 1, 0};
-        Mk.boxes[blockIdx.x + a.first_gel] = b;
+        Mk.boxes[gel_index] = b;
     }
 }
 
-__global__ void __launch_bounds__(kGelThreads) gel_kernel(GelArgs a) {
-    __shared__ int s_box[6];
-    const GelDev& G = a.gels[blockIdx.x + a.first_gel];
+// every phase of one gel, run by one CTA
+__device__ void gel_run(const GelArgs& a, int gel_index, int* s_box) {
+    const GelDev& G = a.gels[gel_index];
     const Idx I{G.LX, G.LY};
     const int iter = a.iter_arg >= 0 ? a.iter_arg : a.ctl->iter;
     bool active = true;
@@ -466,15 +466,28 @@ __global__ void __launch_bounds__(kGelThreads) gel_kernel(GelArgs a) {
         record_center(G, I, iter);
         __syncthreads();
     }
-    if (a.phases & kPhGather) gather(G, a, s_box);
+    if (a.phases & kPhGather) gather(G, a, gel_index, s_box);
+}
+
+__global__ void __launch_bounds__(kGelThreads) gel_kernel(GelArgs a) {
+    __shared__ int s_box[6];
+    gel_run(a, blockIdx.x + a.first_gel, s_box);
+}
+
+// batched: CTA b runs gel entries[b].first_gel of the system described by entries[b]
+__global__ void __launch_bounds__(kGelThreads) gel_batch_kernel(const GelArgs* entries, int n) {
+    __shared__ int s_box[6];
+    if ((int)blockIdx.x >= n) return;
+    const GelArgs& a = entries[blockIdx.x];
+    gel_run(a, a.first_gel, s_box);
 }
 
 // ---------------------------------------------------------------------------
 // concentration exchange at the markers (one warp per marker)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) conc_markers_kernel(MarkerArgs a) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int l = blockIdx.x * 8 + warp;
+// one warp: marker l of the system described by a
+__device__ void conc_marker(const MarkerArgs& a, int l) {
+    const int lane = threadIdx.x & 31;
     const MarkerDev& Mk = a.Mk;
     if (l >= Mk.M) return;
     const int4 b = Mk.base[l];
@@ -516,15 +529,33 @@ _Pragma("unroll")
         if (ok[j]) atomicAdd(&a.source[cell[j]], Sl * (w[j] * scale));
 }
 
+__global__ void __launch_bounds__(256) conc_markers_kernel(MarkerArgs a) {
+    conc_marker(a, blockIdx.x * 8 + (threadIdx.x >> 5));
+}
+
+// batched: warp w belongs to the system whose [first, next) warp range holds it;
+// pairs[2 s + c] are system s's arguments with concentration buffer c, and
+// dyn[s].cur selects the current one
+__global__ void __launch_bounds__(256) conc_markers_batch_kernel(const MarkerArgs* pairs, const SysDyn* dyn,
+                                                                 const int* warp_offsets, int n) {
+    const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (n <= 0 || w >= warp_offsets[n]) return;
+    int lo = 0, hi = n;  // last system with warp_offsets[s] <= w
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (warp_offsets[mid] <= w) lo = mid; else hi = mid;
+    }
+    conc_marker(pairs[2 * lo + dyn[lo].cur], w - warp_offsets[lo]);
+}
+
 // ---------------------------------------------------------------------------
 // repulsion between markers of different gels (shared-memory tiles)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) repulsion_kernel(RepulsionArgs a) {
-    __shared__ float4 s_pos[256];
-    __shared__ int s_own[256];
+// markers [256 b, 256 b + 256) of the system described by a
+__device__ void repulsion_block(const RepulsionArgs& a, int b, float4* s_pos, int* s_own) {
     const MarkerDev& Mk = a.Mk;
     const int M = Mk.M;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = b * blockDim.x + threadIdx.x;
     const float rcut = 2.5f * a.gamma, rc2 = rcut * rcut, sig2 = a.gamma * a.gamma;
     float4 pi = make_float4(0, 0, 0, 0);
     int oi = -1;
@@ -566,6 +597,26 @@ __global__ void __launch_bounds__(256) repulsion_kernel(RepulsionArgs a) {
     }
 }
 
+__global__ void __launch_bounds__(256) repulsion_kernel(RepulsionArgs a) {
+    __shared__ float4 s_pos[256];
+    __shared__ int s_own[256];
+    repulsion_block(a, blockIdx.x, s_pos, s_own);
+}
+
+// batched: block b belongs to the system whose [first, next) block range holds it
+__global__ void __launch_bounds__(256) repulsion_batch_kernel(const RepulsionArgs* systems, const int* block_offsets,
+                                                              int n) {
+    __shared__ float4 s_pos[256];
+    __shared__ int s_own[256];
+    const int b = blockIdx.x;
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (block_offsets[mid] <= b) lo = mid; else hi = mid;
+    }
+    if (n > 0 && b < block_offsets[n]) repulsion_block(systems[lo], b - block_offsets[lo], s_pos, s_own);
+}
+
 // Coupler::scatterToGels: un_robin -= Sl and Fn_robin -= Frep at each marker's node
 __global__ void scatter_kernel(GelDev* gels, MarkerDev Mk) {
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
@@ -595,6 +646,26 @@ cudaError_t launch_conc_markers(const MarkerArgs& a, cudaStream_t s) {
 cudaError_t launch_repulsion(const RepulsionArgs& a, cudaStream_t s) {
     if (a.Mk.M <= 0) return cudaSuccess;
     repulsion_kernel<<<(a.Mk.M + 255) / 256, 256, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gel_batch(const GelArgs* entries, int n, int grid, cudaStream_t s) {
+    if (grid <= 0) return cudaSuccess;
+    gel_batch_kernel<<<grid, kGelThreads, 0, s>>>(entries, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_conc_markers_batch(const MarkerArgs* pairs, const SysDyn* dyn, const int* warp_offsets, int n,
+                                      int warps, cudaStream_t s) {
+    if (warps <= 0) return cudaSuccess;
+    conc_markers_batch_kernel<<<(warps + 7) / 8, 256, 0, s>>>(pairs, dyn, warp_offsets, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_repulsion_batch(const RepulsionArgs* systems, const int* block_offsets, int n, int blocks,
+                                   cudaStream_t s) {
+    if (blocks <= 0) return cudaSuccess;
+    repulsion_batch_kernel<<<blocks, 256, 0, s>>>(systems, block_offsets, n);
     return cudaGetLastError();
 }
 

@@ -46,5 +46,11 @@ cudaError_t launch_gel(const GelArgs& a, int n_gels, cudaStream_t s);
 cudaError_t launch_conc_markers(const MarkerArgs& a, cudaStream_t s);
 cudaError_t launch_repulsion(const RepulsionArgs& a, cudaStream_t s);
 cudaError_t launch_scatter(GelDev* gels, const MarkerDev& Mk, cudaStream_t s);
+// batched forms over several systems (device arrays of per-system arguments)
+cudaError_t launch_gel_batch(const GelArgs* entries, int n, int grid, cudaStream_t s);
+cudaError_t launch_conc_markers_batch(const MarkerArgs* pairs, const SysDyn* dyn, const int* warp_offsets, int n,
+                                      int warps, cudaStream_t s);
+cudaError_t launch_repulsion_batch(const RepulsionArgs* systems, const int* block_offsets, int n, int blocks,
+                                   cudaStream_t s);
 
 }  // namespace glsm

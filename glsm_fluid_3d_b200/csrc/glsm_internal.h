@@ -37,6 +37,14 @@ struct Ctl {
     int pad[2];
 };
 
+// Per-system state of a batch that changes every iteration, kept on the device
+// so that a captured batch iteration replays without host work.
+struct SysDyn {
+    int parity0;  // AA parity at the start of the current iteration
+    int cur;      // current concentration buffer
+    int pad[2];
+};
+
 // One gel: FP64 state in the reference's layout (src/gel.cu:66-114):
 // elements over (LX+1)(LY+1)(LZ+1) slots, nodes over (LX+2)(LY+2)(LZ+2) slots,
 // node vectors as double3 AoS.

@@ -534,20 +534,136 @@ __global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// batched substep: several systems in one persistent launch
+// ---------------------------------------------------------------------------
+struct BatchSlot {
+    TileSlot ts;     // global ticket and the tile's marker boxes
+    int sys;         // system index
+    unsigned local;  // IBM task or tile index within the system
+    int is_ibm;
+    int parity;
+    StepArgs a;      // the system's arguments for this substep
+};
+
+__device__ __forceinline__ int find_sys(const int* offsets, int n, unsigned t) {
+    int lo = 0, hi = n;  // the last s with offsets[s] <= t
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if ((unsigned)offsets[mid] <= t) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// warp 0: resolve global ticket t to (system, local work) and prepare the slot
+__device__ void prepare_batch_slot(const BatchLaunch& L, unsigned t, BatchSlot& sl) {
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned n_ibm_all = (unsigned)L.ibm_offsets[L.n];
+    const unsigned total = n_ibm_all + (unsigned)L.tile_offsets[L.n];
+    int nb = 0;
+    if (t < total) {
+        const bool ibm = t < n_ibm_all;
+        const int s = ibm ? find_sys(L.ibm_offsets, L.n, t) : find_sys(L.tile_offsets, L.n, t - n_ibm_all);
+        const unsigned local = ibm ? t - L.ibm_offsets[s] : (t - n_ibm_all) - L.tile_offsets[s];
+        const int* src = reinterpret_cast<const int*>(&L.sys[s].step);
+        int* dst = reinterpret_cast<int*>(&sl.a);
+        for (int w = lane; w < (int)(sizeof(StepArgs) / 4); w += 32) dst[w] = src[w];
+        __syncwarp();  // the whole copy lands before lane 0 sets the per-launch fields
+        if (lane == 0) {
+            sl.a.k = L.k;
+            sl.a.last = L.last;
+            sl.sys = s;
+            sl.local = local;
+            sl.is_ibm = ibm;
+            sl.parity = (L.sys[s].dyn->parity0 + L.k) & 1;
+        }
+        if (!ibm) {
+            const StepArgs& a = L.sys[s].step;
+            const unsigned c0 = local * kTileCells;
+            const unsigned c1 = min(c0 + kTileCells - 1, (unsigned)a.F.N - 1);
+            const TileExt ext = tile_extent(c0, c1, a.F.nx, a.F.ny, a.div_nx, a.div_nxy);
+            for (int j0 = 0; j0 < a.n_boxes; j0 += 32) {
+                const int j = j0 + (int)lane;
+                Box b{1, 0, 1, 0, 1, 0};
+                bool hit = false;
+                if (j < a.n_boxes) {
+                    b = a.Mk.boxes[j];
+                    hit = b.x0 <= b.x1 && overlaps(b, ext);
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, hit);
+                if (hit) sl.ts.b[nb + __popc(m & ((1u << lane) - 1u))] = b;
+                nb += __popc(m);
+            }
+        }
+    }
+    if (lane == 0) {
+        sl.ts.t = t;
+        sl.ts.nb = nb;
+    }
+}
+
+template <int ST>
+__device__ __forceinline__ void batch_tile(const BatchSlot& sl) {
+    if (!sl.parity)
+        lbm_tile<ST, 0, 0>(sl.a, sl.local, sl.ts);
+    else if (sl.a.F.per[0])
+        lbm_tile<ST, 1, 1>(sl.a, sl.local, sl.ts);
+    else
+        lbm_tile<ST, 1, 0>(sl.a, sl.local, sl.ts);
+}
+
+// Tickets: first every system's IBM tasks, then every system's tiles, so the
+// forward-progress argument of lbm_substep_kernel carries over (a tile waits
+// only for IBM tasks of its own system, all of which have lower tickets).
+__global__ void __launch_bounds__(kTile, 3) lbm_substep_batch_kernel(BatchLaunch L) {
+    __shared__ BatchSlot s_slot[2];
+    const unsigned total = (unsigned)(L.ibm_offsets[L.n] + L.tile_offsets[L.n]);
+    const bool warp0 = threadIdx.x < 32;
+    if (warp0) {
+        unsigned t0 = 0;
+        if (threadIdx.x == 0) t0 = atomicAdd(&L.tickets[L.k], 1u);
+        t0 = __shfl_sync(0xffffffffu, t0, 0);
+        prepare_batch_slot(L, t0, s_slot[0]);
+    }
+    __syncthreads();
+    for (int j = 0;; j ^= 1) {
+        const BatchSlot& sl = s_slot[j];
+        if (sl.ts.t >= total) break;
+        unsigned tn = 0;
+        if (threadIdx.x == 0) tn = atomicAdd(&L.tickets[L.k], 1u);
+        if (sl.is_ibm) {
+            ibm_task(sl.a, sl.local);
+        } else {
+            const int st = sl.a.F.storage;
+            if (st == kStoreF32)
+                batch_tile<kStoreF32>(sl);
+            else if (st == kStoreF16)
+                batch_tile<kStoreF16>(sl);
+            else
+                batch_tile<kStoreBF16>(sl);
+        }
+        if (warp0) {
+            tn = __shfl_sync(0xffffffffu, tn, 0);
+            prepare_batch_slot(L, tn, s_slot[j ^ 1]);
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
 // upwind advection + diffusion of the concentration (once per iteration)
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kTile) conv_diff_kernel(ConcArgs a) {
-    __shared__ int s_nb;
-    __shared__ Box s_b[kMaxBoxes];
+// one 256-cell tile of the upwind advection + diffusion
+__device__ void conv_diff_tile(const ConcArgs& a, unsigned block, Box* s_b, int* s_nb_p) {
+    int& s_nb = *s_nb_p;
     if (threadIdx.x == 0) {
         s_nb = 0;
-        if (a.bump_iter && blockIdx.x == 0) a.ctl->iter += 1;  // nothing in this kernel reads it
+        if (a.bump_iter && block == 0) a.ctl->iter += 1;  // nothing in this kernel reads it
     }
     __syncthreads();
     const FluidDev& F = a.F;
     const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
     const unsigned N = (unsigned)F.N, nxy = nx * ny;
-    const unsigned c0 = blockIdx.x * kTile;
+    const unsigned c0 = block * kTile;
     const unsigned c1 = min(c0 + kTile - 1, N - 1);
     const TileExt ext = tile_extent(c0, c1, nx, ny, a.div_nx, a.div_nxy);
     const int nb = tile_boxes(a.Mk.boxes, a.n_boxes, ext, s_b, &s_nb);
@@ -591,6 +707,45 @@ __global__ void __launch_bounds__(kTile) conv_diff_kernel(ConcArgs a) {
         __stcg(&F.source[i], 0.f);
     }
     c2p[i] = c + F.dtc * (conv + diff + src);
+}
+
+__global__ void __launch_bounds__(kTile) conv_diff_kernel(ConcArgs a) {
+    __shared__ int s_nb;
+    __shared__ Box s_b[kMaxBoxes];
+    conv_diff_tile(a, blockIdx.x, s_b, &s_nb);
+}
+
+__device__ __forceinline__ int find_system(const int* offsets, int n, unsigned t) {
+    int lo = 0, hi = n;  // the last s with offsets[s] <= t
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if ((unsigned)offsets[mid] <= t) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// batched: block b belongs to the system whose [first, next) block range holds
+// it; the system's current concentration buffer comes from its SysDyn
+__global__ void __launch_bounds__(kTile) conv_diff_batch_kernel(const BatchSys* sys, const int* block_offsets, int n) {
+    __shared__ int s_nb;
+    __shared__ Box s_b[kMaxBoxes];
+    const unsigned b = blockIdx.x;
+    if (n == 0 || b >= (unsigned)block_offsets[n]) return;
+    const int s = find_system(block_offsets, n, b);
+    ConcArgs a = sys[s].conc;
+    a.cur = sys[s].dyn->cur;
+    conv_diff_tile(a, b - block_offsets[s], s_b, &s_nb);
+}
+
+// end of a batch iteration: advance every system's iteration, AA parity and
+// concentration buffer
+__global__ void batch_advance_kernel(const BatchSys* sys, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    sys[i].step.ctl->iter += 1;
+    SysDyn* d = sys[i].dyn;
+    d->parity0 ^= (sys[i].step.F.nsub & 1);
+    d->cur ^= 1;
 }
 
 // ---------------------------------------------------------------------------
@@ -670,6 +825,31 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
     }
 #undef GLSM_SUB
     return cudaGetLastError();
+}
+
+cudaError_t launch_substep_batch(const BatchLaunch& L, int grid, cudaStream_t s) {
+    lbm_substep_batch_kernel<<<grid, kTile, 0, s>>>(L);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_conv_diff_batch(const BatchSys* sys, const int* block_offsets, int n, int blocks, cudaStream_t s) {
+    if (blocks <= 0) return cudaSuccess;
+    conv_diff_batch_kernel<<<blocks, kTile, 0, s>>>(sys, block_offsets, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_batch_advance(const BatchSys* sys, int n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    batch_advance_kernel<<<(n + 127) / 128, 128, 0, s>>>(sys, n);
+    return cudaGetLastError();
+}
+
+int batch_resident_ctas() {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_batch_kernel, kTile, 0);
+    return max(1, sms * max(1, per_sm));
 }
 
 cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s) {

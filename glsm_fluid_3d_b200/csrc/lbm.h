@@ -31,7 +31,29 @@ struct ConcArgs {
     FastDiv div_nx, div_nxy;
 };
 
+// one system of a batch (device array, written when the batch changes)
+struct BatchSys {
+    StepArgs step;  // iter_arg < 0: the iteration comes from step.ctl
+    ConcArgs conc;  // cur is replaced by dyn->cur
+    SysDyn* dyn;
+};
+
+// one batched substep launch
+struct BatchLaunch {
+    const BatchSys* sys;
+    const int* ibm_offsets;   // [n + 1] prefix sums of IBM tasks per system
+    const int* tile_offsets;  // [n + 1] prefix sums of lattice tiles per system
+    unsigned* tickets;        // [nsub] batch-wide ticket counters
+    int n;
+    int k;
+    int last;
+};
+
 int lbm_grid(const StepArgs& a);
+cudaError_t launch_substep_batch(const BatchLaunch& L, int grid, cudaStream_t s);
+cudaError_t launch_conv_diff_batch(const BatchSys* sys, const int* block_offsets, int n, int blocks, cudaStream_t s);
+cudaError_t launch_batch_advance(const BatchSys* sys, int n, cudaStream_t s);
+int batch_resident_ctas();
 int lbm_resident_ctas();
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s);
 cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s);

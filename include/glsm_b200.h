@@ -143,6 +143,10 @@ int glsm_gel_build_tube_mask(glsm_gel g, int wall_thickness, int circular);
 /* the drivers' delayed start (src/sim_array.cpp:86-103) for glsm_fluid_run:
  * the gel is skipped before `iter` and fires its pulse at `iter` (0: always on) */
 int glsm_gel_set_active_from(glsm_gel g, int iter);
+/* GelParams::f (the BZ stoichiometric factor, src/gel.cu:634): sets f, recomputes
+ * the steady state by bisection and restarts the interior chemistry from it, as
+ * the reference's constructor does for its fixed f.  Call before stepping. */
+int glsm_gel_set_bz_f(glsm_gel g, double f);
 /* seeded uniform noise in [-amplitude, amplitude) added to um and vm of the
  * interior elements (splitmix64 keyed by seed, gel id, slot, field) */
 int glsm_gel_add_noise(glsm_gel g, uint64_t seed, double amplitude);
@@ -200,6 +204,25 @@ int glsm_fluid_info(glsm_fluid f, int64_t out[8]);
 int glsm_fluid_profile_velocity(glsm_fluid f, int iter, float* ms);
 /* gel_to_lbm_vel and lbm_to_gel_vel (src/fluid.cu:221-222) */
 int glsm_fluid_units(glsm_fluid f, float out[2]);
+
+/* ---- Batch: several systems advanced together -----------------------------
+ * No single counterpart in the reference (which runs one system per process);
+ * this is the serving form of Fluid::stepVelocity & co.  Systems (fluid handles
+ * with their coupler and gels) of any lattice size and gel count join a batch;
+ * glsm_batch_run advances every member by n whole coupled iterations, each one
+ * a CUDA graph of batched launches (one persistent launch per substep for all
+ * members).  All members need the same nsub.  While in a batch a system cannot
+ * be stepped on its own; reads wait for the batch.  Membership changes
+ * re-capture the graph at the next run. */
+typedef struct glsm_batch_s* glsm_batch;
+int glsm_batch_create(glsm_batch* out);
+int glsm_batch_destroy(glsm_batch b);
+/* f enters the batch; its next iteration number is iter0 */
+int glsm_batch_add(glsm_batch b, glsm_fluid f, int iter0);
+int glsm_batch_remove(glsm_batch b, glsm_fluid f);
+int glsm_batch_size(glsm_batch b);
+int glsm_batch_run(glsm_batch b, int n);
+int glsm_batch_sync(glsm_batch b);
 
 /* ---- Substep without device allocation ------------------------------------
  * No counterpart in the reference: an extra entry point for callers that cannot
