@@ -294,9 +294,13 @@ class Batch:
         self.h = h
         self.members = []
 
-    def add(self, fluid, iter0=0):
-        check(self.L.glsm_batch_add(self.h, fluid.h, int(iter0)), "batch add")
+    def add(self, fluid, iter0=0, n_iters=0):
+        """fluid joins at iteration iter0 and runs n_iters iterations (0: no limit)."""
+        check(self.L.glsm_batch_add(self.h, fluid.h, int(iter0), int(n_iters)), "batch add")
         self.members.append(fluid)
+
+    def remaining(self, fluid):
+        return self.L.glsm_batch_remaining(self.h, fluid.h)
 
     def remove(self, fluid):
         check(self.L.glsm_batch_remove(self.h, fluid.h), "batch remove")

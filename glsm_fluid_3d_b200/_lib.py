@@ -73,7 +73,7 @@ def lib():
         "glsm_gel_set_bz_f": [vp, d],
         "glsm_batch_create": [P(vp)],
         "glsm_batch_destroy": [vp],
-        "glsm_batch_add": [vp, vp, i],
+        "glsm_batch_add": [vp, vp, i, i],
         "glsm_batch_remove": [vp, vp],
         "glsm_batch_size": [vp],
         "glsm_batch_run": [vp, i],
@@ -87,6 +87,8 @@ def lib():
     L.glsm_gel_field_size.restype = ctypes.c_size_t
     L.glsm_gel_device_ptr.argtypes = [vp, i]
     L.glsm_gel_device_ptr.restype = vp
+    L.glsm_batch_remaining.argtypes = [vp, vp]
+    L.glsm_batch_remaining.restype = ctypes.c_longlong
     L.glsm_coupler_stream.argtypes = [vp]
     L.glsm_coupler_stream.restype = vp
     _lib = L

@@ -1175,10 +1175,12 @@ int glsm_fluid_write(glsm_fluid f, int field, const float* src, size_t count) {
 // ===========================================================================
 struct glsm_batch_s {
     std::vector<glsm_fluid_s*> sys;
+    std::vector<long long> remaining;  // host mirror of SysDyn::remaining (< 0: no limit)
     int nsub = 0;
     cudaStream_t stream = nullptr, side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     void* arena = nullptr;
+    size_t arena_bytes = 0;
     BatchSys* d_sys = nullptr;
     SysDyn* d_dyn = nullptr;
     GelArgs* d_gel = nullptr;
@@ -1201,8 +1203,6 @@ static int batch_wait(glsm_fluid f) {
 static void batch_free_device(glsm_batch_s* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
-    if (b->arena) cudaFree(b->arena);
-    b->arena = nullptr;
 }
 
 // device descriptors of the current members; recapture of the iteration graph
@@ -1227,9 +1227,10 @@ static int batch_rebuild(glsm_batch_s* b) {
                               make_fastdiv((unsigned)(f->F.nx * f->F.ny))};
         hd[i].parity0 = (int)(f->substeps & 1);
         hd[i].cur = f->cur;
+        hd[i].remaining = (int)std::min<long long>(b->remaining[i], 1 << 30);
         for (int cb = 0; cb < 2; cb++)
             hm[2 * i + cb] = MarkerArgs{c->d_gels, c->mk, f->F.c[cb], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 1};
-        hr[i] = RepulsionArgs{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 1};
+        hr[i] = RepulsionArgs{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 1, nullptr};
         const int phases = kPhElastic | kPhChem | kPhRecord | kPhGather | kPhAuto;
         for (int g = 0; g < (int)c->gels.size(); g++) {
             GelArgs ga = coupler_gel_args(c, phases, -1);
@@ -1259,7 +1260,13 @@ static int batch_rebuild(glsm_batch_s* b) {
         cv.take<unsigned>((size_t)n * b->nsub);
         bytes = align_up(cv.off, 256);
     }
-    CK(cudaMalloc(&b->arena, bytes));
+    if (bytes > b->arena_bytes) {  // grow only
+        if (b->arena) cudaFree(b->arena);
+        b->arena = nullptr;
+        b->arena_bytes = 0;
+        CK(cudaMalloc(&b->arena, bytes * 2));
+        b->arena_bytes = bytes * 2;
+    }
     Carver cv{(char*)b->arena};
     b->d_sys = cv.take<BatchSys>(n);
     b->d_dyn = cv.take<SysDyn>(n);
@@ -1277,6 +1284,12 @@ static int batch_rebuild(glsm_batch_s* b) {
         hs[i].dyn = b->d_dyn + i;
         hs[i].step.ibm_done = b->d_ibm_done + (size_t)i * b->nsub;
         hs[i].step.tickets = b->d_tickets;
+        hr[i].dyn = b->d_dyn + i;
+    }
+    {
+        size_t gi = 0;
+        for (int i = 0; i < n; i++)
+            for (size_t g = 0; g < b->sys[i]->c->gels.size(); g++) hg[gi++].dyn = b->d_dyn + i;
     }
     CK(cudaMemcpy(b->d_sys, hs.data(), n * sizeof(BatchSys), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b->d_dyn, hd.data(), n * sizeof(SysDyn), cudaMemcpyHostToDevice));
@@ -1335,7 +1348,7 @@ int glsm_batch_create(glsm_batch* out) {
     return GLSM_OK;
 }
 
-int glsm_batch_add(glsm_batch b, glsm_fluid f, int iter0) {
+int glsm_batch_add(glsm_batch b, glsm_fluid f, int iter0, int n_iters) {
     if (!b || !f || iter0 < 0) return fail(GLSM_ERR_ARG, "bad argument");
     if (f->batch) return fail(GLSM_ERR_STATE, "system already in a batch");
     if (!b->sys.empty() && f->F.nsub != b->nsub) return fail(GLSM_ERR_ARG, "all systems of a batch need the same nsub");
@@ -1346,6 +1359,7 @@ int glsm_batch_add(glsm_batch b, glsm_fluid f, int iter0) {
     CK(cudaGetLastError());
     f->batch = b;
     b->sys.push_back(f);
+    b->remaining.push_back(n_iters > 0 ? n_iters : -1);
     b->dirty = true;
     return GLSM_OK;
 }
@@ -1353,7 +1367,9 @@ int glsm_batch_add(glsm_batch b, glsm_fluid f, int iter0) {
 int glsm_batch_remove(glsm_batch b, glsm_fluid f) {
     if (!b || !f || f->batch != b) return fail(GLSM_ERR_ARG, "system is not in this batch");
     CK(cudaStreamSynchronize(b->stream));
-    b->sys.erase(std::find(b->sys.begin(), b->sys.end(), f));
+    const size_t at = std::find(b->sys.begin(), b->sys.end(), f) - b->sys.begin();
+    b->sys.erase(b->sys.begin() + at);
+    b->remaining.erase(b->remaining.begin() + at);
     f->batch = nullptr;
     b->dirty = true;
     return GLSM_OK;
@@ -1369,11 +1385,21 @@ int glsm_batch_run(glsm_batch b, int n) {
     }
     if (b->sys.empty() || n == 0) return GLSM_OK;
     for (int it = 0; it < n; it++) CK(cudaGraphLaunch(b->graph, b->stream));
-    for (auto* f : b->sys) {
-        f->substeps += (long long)n * f->F.nsub;
-        f->cur ^= (n & 1);
+    for (size_t i = 0; i < b->sys.size(); i++) {
+        glsm_fluid_s* f = b->sys[i];
+        long long& rem = b->remaining[i];
+        const long long ran = rem < 0 ? n : std::min<long long>(n, rem);
+        if (rem > 0) rem -= ran;
+        f->substeps += ran * f->F.nsub;
+        f->cur ^= (int)(ran & 1);
     }
     return GLSM_OK;
+}
+
+long long glsm_batch_remaining(glsm_batch b, glsm_fluid f) {
+    if (!b || !f || f->batch != b) return -2;
+    const size_t at = std::find(b->sys.begin(), b->sys.end(), f) - b->sys.begin();
+    return b->remaining[at];
 }
 
 int glsm_batch_sync(glsm_batch b) {
@@ -1396,6 +1422,7 @@ int glsm_batch_destroy(glsm_batch b) {
     cudaStreamSynchronize(b->stream);
     for (auto* f : b->sys) f->batch = nullptr;
     batch_free_device(b);
+    if (b->arena) cudaFree(b->arena);
     cudaEventDestroy(b->ev_fork);
     cudaEventDestroy(b->ev_join);
     cudaStreamDestroy(b->side);

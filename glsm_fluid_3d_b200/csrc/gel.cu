@@ -479,6 +479,7 @@ __global__ void __launch_bounds__(kGelThreads) gel_batch_kernel(const GelArgs* e
     __shared__ int s_box[6];
     if ((int)blockIdx.x >= n) return;
     const GelArgs& a = entries[blockIdx.x];
+    if (a.dyn && a.dyn->remaining == 0) return;
     gel_run(a, a.first_gel, s_box);
 }
 
@@ -545,6 +546,7 @@ __global__ void __launch_bounds__(256) conc_markers_batch_kernel(const MarkerArg
         const int mid = (lo + hi) / 2;
         if (warp_offsets[mid] <= w) lo = mid; else hi = mid;
     }
+    if (dyn[lo].remaining == 0) return;
     conc_marker(pairs[2 * lo + dyn[lo].cur], w - warp_offsets[lo]);
 }
 
@@ -614,7 +616,8 @@ __global__ void __launch_bounds__(256) repulsion_batch_kernel(const RepulsionArg
         const int mid = (lo + hi) / 2;
         if (block_offsets[mid] <= b) lo = mid; else hi = mid;
     }
-    if (n > 0 && b < block_offsets[n]) repulsion_block(systems[lo], b - block_offsets[lo], s_pos, s_own);
+    if (n > 0 && b < block_offsets[n] && !(systems[lo].dyn && systems[lo].dyn->remaining == 0))
+        repulsion_block(systems[lo], b - block_offsets[lo], s_pos, s_own);
 }
 
 // Coupler::scatterToGels: un_robin -= Sl and Fn_robin -= Frep at each marker's node

@@ -23,6 +23,7 @@ struct GelArgs {
     int nx, ny, nz;    // lattice (for the stencil cache)
     float h;
     float g2l;         // gel -> lattice velocity factor
+    const SysDyn* dyn; // batched systems: skip the gel when dyn->remaining == 0
 };
 
 struct MarkerArgs {
@@ -40,6 +41,7 @@ struct RepulsionArgs {
     MarkerDev Mk;
     float delta, gamma;
     int scatter;       // also do Fn_robin -= Frep
+    const SysDyn* dyn; // batched systems: skip when dyn->remaining == 0
 };
 
 cudaError_t launch_gel(const GelArgs& a, int n_gels, cudaStream_t s);

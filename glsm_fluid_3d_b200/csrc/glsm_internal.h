@@ -40,9 +40,10 @@ struct Ctl {
 // Per-system state of a batch that changes every iteration, kept on the device
 // so that a captured batch iteration replays without host work.
 struct SysDyn {
-    int parity0;  // AA parity at the start of the current iteration
-    int cur;      // current concentration buffer
-    int pad[2];
+    int parity0;    // AA parity at the start of the current iteration
+    int cur;        // current concentration buffer
+    int remaining;  // iterations still to run (< 0: no limit); 0: the system idles
+    int pad;
 };
 
 // One gel: FP64 state in the reference's layout (src/gel.cu:66-114):

@@ -542,6 +542,7 @@ struct BatchSlot {
     unsigned local;  // IBM task or tile index within the system
     int is_ibm;
     int parity;
+    int idle;        // the ticket belongs to a system that has finished
     StepArgs a;      // the system's arguments for this substep
 };
 
@@ -563,12 +564,21 @@ __device__ void prepare_batch_slot(const BatchLaunch& L, unsigned t, BatchSlot& 
     if (t < total) {
         const bool ibm = t < n_ibm_all;
         const int s = ibm ? find_sys(L.ibm_offsets, L.n, t) : find_sys(L.tile_offsets, L.n, t - n_ibm_all);
+        if (L.sys[s].dyn->remaining == 0) {  // an idle system: nothing to do for this ticket
+            if (lane == 0) {
+                sl.ts.t = t;
+                sl.ts.nb = 0;
+                sl.idle = 1;
+            }
+            return;
+        }
         const unsigned local = ibm ? t - L.ibm_offsets[s] : (t - n_ibm_all) - L.tile_offsets[s];
         const int* src = reinterpret_cast<const int*>(&L.sys[s].step);
         int* dst = reinterpret_cast<int*>(&sl.a);
         for (int w = lane; w < (int)(sizeof(StepArgs) / 4); w += 32) dst[w] = src[w];
         __syncwarp();  // the whole copy lands before lane 0 sets the per-launch fields
         if (lane == 0) {
+            sl.idle = 0;
             sl.a.k = L.k;
             sl.a.last = L.last;
             sl.sys = s;
@@ -630,7 +640,9 @@ __global__ void __launch_bounds__(kTile, 3) lbm_substep_batch_kernel(BatchLaunch
         if (sl.ts.t >= total) break;
         unsigned tn = 0;
         if (threadIdx.x == 0) tn = atomicAdd(&L.tickets[L.k], 1u);
-        if (sl.is_ibm) {
+        if (sl.idle) {
+            // nothing: the system has run all its requested iterations
+        } else if (sl.is_ibm) {
             ibm_task(sl.a, sl.local);
         } else {
             const int st = sl.a.F.storage;
@@ -732,6 +744,7 @@ __global__ void __launch_bounds__(kTile) conv_diff_batch_kernel(const BatchSys* 
     const unsigned b = blockIdx.x;
     if (n == 0 || b >= (unsigned)block_offsets[n]) return;
     const int s = find_system(block_offsets, n, b);
+    if (sys[s].dyn->remaining == 0) return;
     ConcArgs a = sys[s].conc;
     a.cur = sys[s].dyn->cur;
     conv_diff_tile(a, b - block_offsets[s], s_b, &s_nb);
@@ -742,8 +755,10 @@ __global__ void __launch_bounds__(kTile) conv_diff_batch_kernel(const BatchSys* 
 __global__ void batch_advance_kernel(const BatchSys* sys, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    sys[i].step.ctl->iter += 1;
     SysDyn* d = sys[i].dyn;
+    if (d->remaining == 0) return;
+    if (d->remaining > 0) d->remaining -= 1;
+    sys[i].step.ctl->iter += 1;
     d->parity0 ^= (sys[i].step.F.nsub & 1);
     d->cur ^= 1;
 }

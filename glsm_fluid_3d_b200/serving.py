@@ -134,7 +134,7 @@ class Stats:
 class Server:
     """Admits requests by HBM budget and advances all resident systems together."""
 
-    def __init__(self, budget_bytes: float = 150e9, max_chunk: int = 100, keep_results: bool = False):
+    def __init__(self, budget_bytes: float = 150e9, max_chunk: int = 20, keep_results: bool = False):
         self.budget = budget_bytes
         self.max_chunk = max_chunk
         self.keep_results = keep_results
@@ -155,7 +155,7 @@ class Server:
                 while pending and pending[0].arrival <= now and used + device_bytes(pending[0]) <= self.budget:
                     req = pending.pop(0)
                     s = build_system(req)
-                    batch.add(s.fluid, 0)
+                    batch.add(s.fluid, 0, req.steps)  # the device stops it after req.steps iterations
                     active[req.rid] = [req, s, req.steps]
                     used += device_bytes(req)
                 max_res = max(max_res, len(active))
@@ -163,14 +163,16 @@ class Server:
                     if pending:  # idle until the next arrival
                         time.sleep(max(0.0, pending[0].arrival - (clock() - t0)))
                     continue
-                chunk = min(self.max_chunk, min(v[2] for v in active.values()))
+                # a fixed chunk: members that finish inside it idle until it ends
+                chunk = min(self.max_chunk, max(v[2] for v in active.values()))
                 batch.run(chunk)
                 batch.sync()
                 runs += 1
                 done = []
                 for rid, v in active.items():
-                    v[2] -= chunk
-                    work += v[0].cells * 25.0 * chunk
+                    ran = min(chunk, v[2])
+                    v[2] -= ran
+                    work += v[0].cells * 25.0 * ran
                     if v[2] <= 0:
                         done.append(rid)
                 for rid in done:

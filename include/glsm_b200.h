@@ -217,8 +217,11 @@ int glsm_fluid_units(glsm_fluid f, float out[2]);
 typedef struct glsm_batch_s* glsm_batch;
 int glsm_batch_create(glsm_batch* out);
 int glsm_batch_destroy(glsm_batch b);
-/* f enters the batch; its next iteration number is iter0 */
-int glsm_batch_add(glsm_batch b, glsm_fluid f, int iter0);
+/* f enters the batch; its next iteration number is iter0; it runs n_iters more
+ * iterations (then idles until removed), or without limit when n_iters <= 0 */
+int glsm_batch_add(glsm_batch b, glsm_fluid f, int iter0, int n_iters);
+/* iterations f still has to run in the batch (-1: no limit, -2: not a member) */
+long long glsm_batch_remaining(glsm_batch b, glsm_fluid f);
 int glsm_batch_remove(glsm_batch b, glsm_fluid f);
 int glsm_batch_size(glsm_batch b);
 int glsm_batch_run(glsm_batch b, int n);
