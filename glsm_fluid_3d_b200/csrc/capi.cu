@@ -84,6 +84,7 @@ struct glsm_fluid_s {
     long long substeps = 0;      // AA parity bookkeeping
     float* scratch = nullptr;    // 19*N floats, allocated on first use
     int lbm_ctas = 0;            // resident CTAs of the persistent substep kernel
+    int staged_ctas = 0;         // resident CTAs of the staged substep kernel (0: not used)
     struct glsm_batch_s* batch = nullptr;  // batch this system belongs to
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 };
@@ -794,6 +795,7 @@ static StepArgs step_args(glsm_fluid f, int k, int iter_arg) {
     a.div_nxy = make_fastdiv((unsigned)(f->F.nx * f->F.ny));
     a.n_tiles = (int)((f->F.N + kTileCells - 1) / kTileCells);
     a.lbm_ctas = f->lbm_ctas;
+    a.staged_ctas = f->staged_ctas;
     return a;
 }
 
@@ -833,10 +835,14 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     F.ramp_steps = d->ramp_steps;
     F.nsub = d->nsub;
     const size_t esz = (d->storage == GLSM_STORE_F32) ? 4 : 2;
+    // guard bands before and after the 19 planes: the staged substep kernel
+    // copies whole shifted tile ranges, which for boundary tiles reach up to a
+    // z-plane and a row (plus one tile) beyond the planes
+    const size_t guard = align_up((size_t)d->nx * d->ny + d->nx + 2 * kTileCells + 64, 64);
     size_t bytes;
     {
         Carver cv{nullptr};
-        cv.take<char>(19 * (size_t)F.S * esz);
+        cv.take<char>((19 * (size_t)F.S + 2 * guard) * esz);
         cv.take<float4>(N);
         cv.take<float4>(N);
         for (int i = 0; i < 3; i++) cv.take<float>(N);
@@ -850,7 +856,7 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     }
     f->bytes = bytes;
     Carver cv{(char*)f->arena};
-    F.pop = cv.take<char>(19 * (size_t)F.S * esz);
+    F.pop = cv.take<char>((19 * (size_t)F.S + 2 * guard) * esz) + guard * esz;
     F.u = cv.take<float4>(N);
     F.Fibm = cv.take<float4>(N);
     F.c[0] = cv.take<float>(N);
@@ -872,6 +878,15 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     int nsub_phys;
     fluid_units(d->tau, d->h, c->g2l, c->l2g, nsub_phys);
     f->lbm_ctas = lbm_resident_ctas();
+    {
+        static int ctas32 = -1, ctas16 = -1;  // per process (one device type)
+        if (ctas32 < 0) staged_setup(&ctas32, &ctas16);
+        // the shared-memory staged kernel is kept for measurements; the register
+        // kernel is the default
+        const char* kind = getenv("GLSM_LBM_KERNEL");
+        const bool staged = kind && std::strcmp(kind, "staged") == 0;
+        f->staged_ctas = staged ? (d->storage == GLSM_STORE_F32 ? ctas32 : ctas16) : 0;
+    }
     f->c = c;
     c->fluid = f;
     // the gels' gather now knows the lattice

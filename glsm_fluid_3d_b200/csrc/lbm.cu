@@ -31,14 +31,20 @@ struct PopIO;
 template <>
 struct PopIO<kStoreF32> {
     using T = float;
+    static constexpr bool kScaled = false;
     static __device__ __forceinline__ float ld(const T* p, float) { return *p; }
     static __device__ __forceinline__ void st(T* p, float v, float) { *p = v; }
+    static __device__ __forceinline__ float raw(const T* p) { return *p; }
+    static __device__ __forceinline__ void st_raw(T* p, float v) { *p = v; }
 };
 template <>
 struct PopIO<kStoreF16> {
     using T = __half;
+    static constexpr bool kScaled = true;  // stored value = deviation * scale
     static __device__ __forceinline__ float ld(const T* p, float inv_scale) { return __half2float(*p) * inv_scale; }
     static __device__ __forceinline__ void st(T* p, float v, float scale) { *p = __float2half_rn(v * scale); }
+    static __device__ __forceinline__ float raw(const T* p) { return __half2float(*p); }
+    static __device__ __forceinline__ void st_raw(T* p, float v) { *p = __float2half_rn(v); }
 };
 template <>
 struct PopIO<kStoreBF16> {
@@ -47,6 +53,9 @@ struct PopIO<kStoreBF16> {
         return __bfloat162float(*p) * inv_scale;
     }
     static __device__ __forceinline__ void st(T* p, float v, float scale) { *p = __float2bfloat16_rn(v * scale); }
+    static constexpr bool kScaled = false;  // stored unscaled
+    static __device__ __forceinline__ float raw(const T* p) { return __bfloat162float(*p); }
+    static __device__ __forceinline__ void st_raw(T* p, float v) { *p = __float2bfloat16_rn(v); }
 };
 
 __device__ __forceinline__ int current_iter(int iter_arg, const Ctl* ctl) {
@@ -127,12 +136,12 @@ __device__ __forceinline__ int tile_boxes(const Box* boxes, int n_boxes, const T
 // reference loops).  Interpolates u of the previous substep, forms the penalty
 // force beta_eff (Vl - Ul) and spreads it with vector float atomics.
 // ---------------------------------------------------------------------------
-__device__ void ibm_task(const StepArgs& a, unsigned task) {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+// IBM interpolation and spreading of marker l by one warp
+__device__ __forceinline__ void ibm_marker(const StepArgs& a, int l) {
+    const int lane = threadIdx.x & 31;
     const FluidDev& F = a.F;
     const MarkerDev& Mk = a.Mk;
-    const int l = (int)task * kMarkersPerTask + warp;
-    if (warp < kMarkersPerTask && l < Mk.M) {
+    {
         const float be = beta_eff(F.beta, F.ramp_steps, current_iter(a.iter_arg, a.ctl));
         const int4 b = Mk.base[l];
         const float4 px = Mk.phx[l], py = Mk.phy[l], pz = Mk.phz[l];
@@ -178,6 +187,13 @@ __device__ void ibm_task(const StepArgs& a, unsigned task) {
             }
         }
     }
+}
+
+// one IBM task of a CTA: kMarkersPerTask markers, a warp per marker
+__device__ void ibm_task(const StepArgs& a, unsigned task) {
+    const int warp = threadIdx.x >> 5;
+    const int l = (int)task * kMarkersPerTask + warp;
+    if (warp < kMarkersPerTask && l < a.Mk.M) ibm_marker(a, l);
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
@@ -223,22 +239,29 @@ __device__ __forceinline__ float cdot(float x, float y, float z) {
     else return sgn<CZ>(z);
 }
 
+// The collision works on v = 3u and G = 3F (so that 3 c.u = c.v and 9 (c.u)(c.F)
+// = (c.v)(c.G)) with the weight w of each direction class (faces 1/18,
+// diagonals 1/36) and the storage scale folded into per-class constants:
+//   deq_q + F_q (even part) = cv (ae cv + h) + K,   odd part = aod cv + h
+//   ae = w omega rho / 2, aod = w omega rho, h = w fp cG,
+//   K = w (omega (drho - rho uu 3/2) - 3 fp uF)
 struct CollideTerms {
-    float ux, uy, uz, Fx, Fy, Fz, even0, force0, rho45, rho3, fp9, fp3, omega;
+    float vx, vy, vz, Gx, Gy, Gz;
+    float omc;                    // 1 - omega
+    float K[2], ae[2], aod[2], b[2];
 };
 
-// relaxation of the pair (Q, opp(Q)): equilibrium and forcing split into the
-// parts even and odd in c_Q, shared by the pair
 template <int Q>
 __device__ __forceinline__ void collide_pair(float (&d)[19], const CollideTerms& t) {
     constexpr int O = qopp(Q);
-    constexpr float w = qw(Q);
-    const float cu = cdot<qcx(Q), qcy(Q), qcz(Q)>(t.ux, t.uy, t.uz);
-    const float cF = cdot<qcx(Q), qcy(Q), qcz(Q)>(t.Fx, t.Fy, t.Fz);
-    const float ev = fmaf(t.rho45 * cu, cu, t.even0), od = t.rho3 * cu;
-    const float fe = fmaf(t.fp9 * cu, cF, t.force0), fo = t.fp3 * cF;
-    d[Q] = fmaf(t.omega, fmaf(w, ev + od, -d[Q]), fmaf(w, fe + fo, d[Q]));
-    d[O] = fmaf(t.omega, fmaf(w, ev - od, -d[O]), fmaf(w, fe - fo, d[O]));
+    constexpr int C = (Q <= 6) ? 0 : 1;  // direction class
+    const float cv = cdot<qcx(Q), qcy(Q), qcz(Q)>(t.vx, t.vy, t.vz);
+    const float cG = cdot<qcx(Q), qcy(Q), qcz(Q)>(t.Gx, t.Gy, t.Gz);
+    const float h = t.b[C] * cG;
+    const float Od = fmaf(t.aod[C], cv, h);
+    const float E = fmaf(fmaf(t.ae[C], cv, h), cv, t.K[C]);
+    d[Q] = fmaf(t.omc, d[Q], E + Od);
+    d[O] = fmaf(t.omc, d[O], E - Od);
 }
 
 template <int Q>
@@ -255,9 +278,12 @@ __device__ __forceinline__ void moment_pair(const float (&d)[19], float& drho, f
 // d_q <- d_q + omega (deq_q - d_q) + F_q with
 //   deq_q = w_q (drho + rho (3 cu + 4.5 cu^2 - 1.5 uu))
 //   F_q   = w_q (1 - 1/(2 tau)) (3 cF + 9 cu cF - 3 uF)
-// The first members of the nine (q, opp q) pairs: 1 3 5 7 8 11 12 15 16.
-__device__ __forceinline__ void collide(float (&d)[19], float Fx, float Fy, float Fz, float omega, float fp,
-                                        float& ux, float& uy, float& uz, float& rho) {
+// d holds deviations times the storage scale when SCALED (inv = 1/scale); Fh is
+// half the body force.  The first members of the nine (q, opp q) pairs:
+// 1 3 5 7 8 11 12 15 16.
+template <bool SCALED>
+__device__ __forceinline__ void collide(float (&d)[19], float Fhx, float Fhy, float Fhz, float omega, float fp,
+                                        float inv, float scale, float& ux, float& uy, float& uz, float& rho) {
     float drho = d[0], jx = 0.f, jy = 0.f, jz = 0.f;
     moment_pair<1>(d, drho, jx, jy, jz);
     moment_pair<3>(d, drho, jx, jy, jz);
@@ -268,28 +294,40 @@ __device__ __forceinline__ void collide(float (&d)[19], float Fx, float Fy, floa
     moment_pair<12>(d, drho, jx, jy, jz);
     moment_pair<15>(d, drho, jx, jy, jz);
     moment_pair<16>(d, drho, jx, jy, jz);
+    if (SCALED) {
+        drho *= inv;
+        jx *= inv;
+        jy *= inv;
+        jz *= inv;
+    }
     rho = 1.0f + drho;
-    const float inv = __frcp_rn(rho);
-    ux = (jx + 0.5f * Fx) * inv;
-    uy = (jy + 0.5f * Fy) * inv;
-    uz = (jz + 0.5f * Fz) * inv;
-    const float uu = ux * ux + uy * uy + uz * uz;
-    const float uF = ux * Fx + uy * Fy + uz * Fz;
+    const float ir = __frcp_rn(rho);
+    ux = (jx + Fhx) * ir;
+    uy = (jy + Fhy) * ir;
+    uz = (jz + Fhz) * ir;
     CollideTerms t;
-    t.ux = ux;
-    t.uy = uy;
-    t.uz = uz;
-    t.Fx = Fx;
-    t.Fy = Fy;
-    t.Fz = Fz;
-    t.even0 = drho - 1.5f * rho * uu;  // deq / w without the c terms
-    t.force0 = -3.0f * fp * uF;         // F / w without the c terms
-    t.rho45 = 4.5f * rho;
-    t.rho3 = 3.0f * rho;
-    t.fp9 = 9.0f * fp;
-    t.fp3 = 3.0f * fp;
-    t.omega = omega;
-    d[0] = fmaf(omega, fmaf(qw(0), t.even0, -d[0]), fmaf(qw(0), t.force0, d[0]));
+    t.vx = 3.0f * ux;
+    t.vy = 3.0f * uy;
+    t.vz = 3.0f * uz;
+    t.Gx = 6.0f * Fhx;
+    t.Gy = 6.0f * Fhy;
+    t.Gz = 6.0f * Fhz;
+    t.omc = 1.0f - omega;
+    const float vv = t.vx * t.vx + t.vy * t.vy + t.vz * t.vz;  // 9 uu
+    const float vG = t.vx * t.Gx + t.vy * t.Gy + t.vz * t.Gz;  // 9 uF
+    const float wr = SCALED ? omega * rho * scale : omega * rho;
+    const float sfp = SCALED ? fp * scale : fp;
+    // omega (drho - 1.5 rho uu) - 3 fp uF, times the scale
+    const float K1 = fmaf(-(1.0f / 6.0f) * wr, vv, fmaf(-(1.0f / 3.0f) * sfp, vG, (SCALED ? omega * scale : omega) * drho));
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        const float w = c == 0 ? qw(1) : qw(7);
+        t.K[c] = w * K1;
+        t.aod[c] = w * wr;
+        t.ae[c] = (0.5f * w) * wr;
+        t.b[c] = w * sfp;
+    }
+    d[0] = fmaf(t.omc, d[0], qw(0) * K1);
     collide_pair<1>(d, t);
     collide_pair<3>(d, t);
     collide_pair<5>(d, t);
@@ -301,94 +339,41 @@ __device__ __forceinline__ void collide(float (&d)[19], float Fx, float Fy, floa
     collide_pair<16>(d, t);
 }
 
-// one cell of a substep: gather (AA pattern), collide, scatter
+// force, collision and AA-pattern scatter of one cell (shared by the register
+// and the shared-memory staged gathers)
 template <int ST, int PARITY, int PERX>
-__device__ __forceinline__ void lbm_cell(const StepArgs& a, unsigned i, bool inb) {
+__device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, unsigned x, unsigned y, unsigned z,
+                                                bool fast, bool xin, bool inb, float (&d)[19]) {
     using IO = PopIO<ST>;
     using T = typename IO::T;
     const FluidDev& F = a.F;
     const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
     const unsigned S = (unsigned)F.S, nxy = nx * ny;
-    const unsigned z = fdiv(i, a.div_nxy);
-    const unsigned rem = i - z * nxy;
-    const unsigned y = fdiv(rem, a.div_nx);
-    const unsigned x = rem - y * nx;
     T* P = reinterpret_cast<T*>(F.pop);
-    const float isc = F.inv_scale;
-    float d[19];
-    // odd substeps: a warp whose cells are all off the y and z boundary planes
-    // streams with constant neighbour offsets (x walls or wraps per lane);
-    // other warps take the general path
-    bool fast = true;
-    if (PARITY == 1) fast = __all_sync(__activemask(), (y - 1u < ny - 2u) && (z - 1u < nz - 2u));
-    if (PARITY == 0) {
-#pragma unroll
-        for (int q = 0; q < 19; q++) d[q] = IO::ld(P + (q * S + i), isc);
-    } else if (fast) {
-#pragma unroll
-        for (int q = 0; q < 19; q++) {
-            // arriving f_q(x) = post-collision f_q(x - c_q), in slot opp(q) at x - c_q;
-            // across a wall it is the bounced opp(q) population of x, in slot q at x
-            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
-            const unsigned nbr = i - (unsigned)(cx + cy * (int)nx + cz * (int)nxy);
-            if (cx == 0) {
-                d[q] = IO::ld(P + (qopp(q) * S + nbr), isc);
-            } else {
-                const bool edge = (cx > 0) ? (x == 0) : (x == nx - 1);
-                if (PERX)
-                    d[q] = IO::ld(P + (qopp(q) * S + (edge ? nbr + (unsigned)(cx * (int)nx) : nbr)), isc);
-                else
-                    d[q] = IO::ld(P + (edge ? q * S + i : qopp(q) * S + nbr), isc);
-            }
-        }
-    } else {
-        int mo[3], po[3];
-        bool mw[3], pw[3];
-        const unsigned c[3] = {x, y, z}, n[3] = {nx, ny, nz}, st[3] = {1u, nx, nxy};
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            mw[k] = pw[k] = false;
-            mo[k] = -(int)st[k];
-            po[k] = (int)st[k];
-            if (c[k] == 0) {
-                if (F.per[k]) mo[k] = (int)((n[k] - 1) * st[k]);
-                else mw[k] = true;
-            }
-            if (c[k] == n[k] - 1) {
-                if (F.per[k]) po[k] = -(int)((n[k] - 1) * st[k]);
-                else pw[k] = true;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 19; q++) {
-            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
-            const bool wall = (cx > 0 && mw[0]) || (cx < 0 && pw[0]) || (cy > 0 && mw[1]) || (cy < 0 && pw[1]) ||
-                              (cz > 0 && mw[2]) || (cz < 0 && pw[2]);
-            const int off = (cx > 0 ? mo[0] : cx < 0 ? po[0] : 0) + (cy > 0 ? mo[1] : cy < 0 ? po[1] : 0) +
-                            (cz > 0 ? mo[2] : cz < 0 ? po[2] : 0);
-            d[q] = IO::ld(P + (wall ? q * S + i : qopp(q) * S + i + (unsigned)off), isc);
-        }
-    }
-
-    // body force: uniform F_const plus the IBM force inside the marker boxes
-    float Fx = F.Fc[0], Fy = F.Fc[1], Fz = F.Fc[2];
+    const long long LS = S, Lnx = nx, Lnxy = nxy;
+    // half the body force: uniform F_const plus the IBM force inside the marker boxes
+    float Fx = 0.5f * F.Fc[0], Fy = 0.5f * F.Fc[1], Fz = 0.5f * F.Fc[2];
     if (inb) {
         const float4 fi = __ldcg(&F.Fibm[i]);
-        Fx += fi.x;
-        Fy += fi.y;
-        Fz += fi.z;
+        Fx = fmaf(0.5f, fi.x, Fx);
+        Fy = fmaf(0.5f, fi.y, Fy);
+        Fz = fmaf(0.5f, fi.z, Fz);
         __stcg(&F.Fibm[i], make_float4(0.f, 0.f, 0.f, 0.f));
     }
     float ux, uy, uz, rho;
-    collide(d, Fx, Fy, Fz, F.omega, F.fpref, ux, uy, uz, rho);
-    // recompute store addresses from an opaque copy of the base pointer instead
-    // of keeping the 19 load addresses alive across the collision
-    asm volatile("mov.b64 %0, %0;" : "+l"(P));
+    collide<IO::kScaled>(d, Fx, Fy, Fz, F.omega, F.fpref, F.inv_scale, F.scale, ux, uy, uz, rho);
 
-    const float sc = F.scale;
+    T* Pi = P + i;
     if (PARITY == 0) {
 #pragma unroll
-        for (int q = 0; q < 19; q++) IO::st(P + (qopp(q) * S + i), d[q], sc);
+        for (int q = 0; q < 19; q++) IO::st_raw(Pi + qopp(q) * LS, d[q]);
+    } else if (fast && xin) {
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            // post-collision f_q(x) streams to x + c_q, slot q
+            const long long off = qcx(q) + qcy(q) * Lnx + qcz(q) * Lnxy;
+            IO::st_raw(Pi + (q * LS + off), d[q]);
+        }
     } else if (fast) {
 #pragma unroll
         for (int q = 0; q < 19; q++) {
@@ -397,13 +382,13 @@ __device__ __forceinline__ void lbm_cell(const StepArgs& a, unsigned i, bool inb
             const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
             const unsigned nbr = i + (unsigned)(cx + cy * (int)nx + cz * (int)nxy);
             if (cx == 0) {
-                IO::st(P + (q * S + nbr), d[q], sc);
+                IO::st_raw(P + (q * S + nbr), d[q]);
             } else {
                 const bool edge = (cx > 0) ? (x == nx - 1) : (x == 0);
                 if (PERX)
-                    IO::st(P + (q * S + (edge ? nbr - (unsigned)(cx * (int)nx) : nbr)), d[q], sc);
+                    IO::st_raw(P + (q * S + (edge ? nbr - (unsigned)(cx * (int)nx) : nbr)), d[q]);
                 else
-                    IO::st(P + (edge ? qopp(q) * S + i : q * S + nbr), d[q], sc);
+                    IO::st_raw(P + (edge ? qopp(q) * S + i : q * S + nbr), d[q]);
             }
         }
     } else {
@@ -431,10 +416,97 @@ __device__ __forceinline__ void lbm_cell(const StepArgs& a, unsigned i, bool inb
                               (cz > 0 && pw[2]) || (cz < 0 && mw[2]);
             const int off = (cx > 0 ? po[0] : cx < 0 ? mo[0] : 0) + (cy > 0 ? po[1] : cy < 0 ? mo[1] : 0) +
                             (cz > 0 ? po[2] : cz < 0 ? mo[2] : 0);
-            IO::st(P + (wall ? qopp(q) * S + i : q * S + i + (unsigned)off), d[q], sc);
+            IO::st_raw(P + (wall ? qopp(q) * S + i : q * S + i + (unsigned)off), d[q]);
         }
     }
     if (inb || a.last) F.u[i] = make_float4(ux, uy, uz, rho);
+}
+
+// one cell of a substep: gather (AA pattern), collide, scatter.  Addresses are a
+// per-thread base pointer (the cell in plane 0) plus per-direction offsets that
+// depend only on the lattice, the same for every lane.
+template <int ST, int PARITY, int PERX>
+__device__ __forceinline__ void lbm_cell(const StepArgs& a, unsigned i, bool inb) {
+    using IO = PopIO<ST>;
+    using T = typename IO::T;
+    const FluidDev& F = a.F;
+    const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
+    const unsigned S = (unsigned)F.S, nxy = nx * ny;
+    const unsigned z = fdiv(i, a.div_nxy);
+    const unsigned rem = i - z * nxy;
+    const unsigned y = fdiv(rem, a.div_nx);
+    const unsigned x = rem - y * nx;
+    const T* Pi = reinterpret_cast<const T*>(F.pop) + i;
+    const long long LS = S, Lnx = nx, Lnxy = nxy;
+    float d[19];
+    // odd substeps: warps whose cells are all off the y and z boundary planes
+    // stream with constant neighbour offsets; among them, warps with no cell on
+    // an x wall need no per-lane choice at all
+    bool fast = true, xin = true;
+    if (PARITY == 1) {
+        const unsigned act = __activemask();
+        fast = __all_sync(act, (y - 1u < ny - 2u) && (z - 1u < nz - 2u));
+        xin = __all_sync(act, x - 1u < nx - 2u);
+    }
+    if (PARITY == 0) {
+#pragma unroll
+        for (int q = 0; q < 19; q++) d[q] = IO::raw(Pi + q * LS);
+    } else if (fast && xin) {
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            // arriving f_q(x) = post-collision f_q(x - c_q), in slot opp(q) at x - c_q
+            const long long off = qcx(q) + qcy(q) * Lnx + qcz(q) * Lnxy;
+            d[q] = IO::raw(Pi + (qopp(q) * LS - off));
+        }
+    } else if (fast) {
+        const T* P = reinterpret_cast<const T*>(F.pop);
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
+            const long long off = cx + cy * Lnx + cz * Lnxy;
+            if (cx == 0) {
+                d[q] = IO::raw(Pi + (qopp(q) * LS - off));
+            } else {
+                // across an x wall: the bounced opp(q) population of x, in slot q
+                // at x; periodic x: the wrapped neighbour
+                const bool edge = (cx > 0) ? (x == 0) : (x == nx - 1);
+                const unsigned nbr = i - (unsigned)off;
+                if (PERX)
+                    d[q] = IO::raw(P + (qopp(q) * S + (edge ? nbr + (unsigned)(cx * (int)nx) : nbr)));
+                else
+                    d[q] = IO::raw(P + (edge ? q * S + i : qopp(q) * S + nbr));
+            }
+        }
+    } else {
+        const T* P = reinterpret_cast<const T*>(F.pop);
+        int mo[3], po[3];
+        bool mw[3], pw[3];
+        const unsigned c[3] = {x, y, z}, n[3] = {nx, ny, nz}, st[3] = {1u, nx, nxy};
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            mw[k] = pw[k] = false;
+            mo[k] = -(int)st[k];
+            po[k] = (int)st[k];
+            if (c[k] == 0) {
+                if (F.per[k]) mo[k] = (int)((n[k] - 1) * st[k]);
+                else mw[k] = true;
+            }
+            if (c[k] == n[k] - 1) {
+                if (F.per[k]) po[k] = -(int)((n[k] - 1) * st[k]);
+                else pw[k] = true;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
+            const bool wall = (cx > 0 && mw[0]) || (cx < 0 && pw[0]) || (cy > 0 && mw[1]) || (cy < 0 && pw[1]) ||
+                              (cz > 0 && mw[2]) || (cz < 0 && pw[2]);
+            const int off = (cx > 0 ? mo[0] : cx < 0 ? po[0] : 0) + (cy > 0 ? mo[1] : cy < 0 ? po[1] : 0) +
+                            (cz > 0 ? mo[2] : cz < 0 ? po[2] : 0);
+            d[q] = IO::raw(P + (wall ? q * S + i : qopp(q) * S + i + (unsigned)off));
+        }
+    }
+    collide_scatter<ST, PARITY, PERX>(a, i, x, y, z, fast, xin, inb, d);
 }
 
 // Per-tile state prepared by warp 0 one tile ahead: the ticket and the marker
@@ -531,6 +603,278 @@ __global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
         }
         __syncthreads();
     }
+}
+
+
+// ---------------------------------------------------------------------------
+// staged substep: each tile's 19 population ranges are brought into shared
+// memory by one-dimensional bulk copies (TMA) one tile ahead of the compute
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// order this thread's (and, after a barrier, the CTA's) generic-proxy accesses
+// to shared memory before the following async-proxy (bulk copy) writes
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+template <int ST>
+struct Stage {
+    using T = typename PopIO<ST>::T;
+    static constexpr int PAD = 16 / (int)sizeof(T);      // one 16-byte vector of elements
+    static constexpr int PLANE = kTileCells + PAD;       // staged elements per direction
+    static constexpr unsigned BYTES = PLANE * sizeof(T); // bytes per direction (a multiple of 16)
+    static constexpr size_t BUF = 19 * (size_t)BYTES;    // one staged tile
+    static constexpr int CTAS = (ST == kStoreF32) ? 2 : 3;
+};
+
+// thread 0: bulk copies of the 19 ranges tile `tile` reads.  For direction q the
+// range starts at the tile's first cell (even substeps, slot q) or at the first
+// cell's upstream neighbour x - c_q (odd substeps, slot opp q), rounded down to
+// 16 bytes; shift[q] is the rounding.  Ranges of boundary tiles may reach into
+// the guard bands around the population array; the lanes that would use such
+// values (walls, wraps) read global memory instead.
+template <int ST, int PARITY>
+__device__ __forceinline__ void issue_tile_loads(const StepArgs& a, unsigned tile, typename Stage<ST>::T* buf,
+                                                 int* shift, unsigned long long* bar) {
+    using T = typename Stage<ST>::T;
+    constexpr int PAD = Stage<ST>::PAD;
+    const FluidDev& F = a.F;
+    const long long S = F.S, nx = F.nx, nxy = (long long)F.nx * F.ny;
+    const long long c0 = (long long)tile * kTileCells;
+    const T* P = reinterpret_cast<const T*>(F.pop);
+    fence_proxy_async_smem();
+    mbar_arrive_expect_tx(bar, 19u * Stage<ST>::BYTES);
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        const long long off = qcx(q) + qcy(q) * nx + qcz(q) * nxy;
+        const long long start = PARITY == 0 ? (long long)q * S + c0 : (long long)qopp(q) * S + c0 - off;
+        const long long al = start & ~(long long)(PAD - 1);
+        shift[q] = (int)(start - al);
+        bulk_copy_g2s(buf + q * Stage<ST>::PLANE, P + al, Stage<ST>::BYTES, bar);
+    }
+}
+
+// gather of one cell from the staged tile (li: the cell's index in the tile)
+template <int ST, int PARITY, int PERX>
+__device__ __forceinline__ void lbm_cell_staged(const StepArgs& a, unsigned i, unsigned li, bool inb,
+                                                const typename Stage<ST>::T* sb, const int* shift) {
+    using IO = PopIO<ST>;
+    using T = typename IO::T;
+    constexpr int PL = Stage<ST>::PLANE;
+    const FluidDev& F = a.F;
+    const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
+    const unsigned S = (unsigned)F.S, nxy = nx * ny;
+    const unsigned z = fdiv(i, a.div_nxy);
+    const unsigned rem = i - z * nxy;
+    const unsigned y = fdiv(rem, a.div_nx);
+    const unsigned x = rem - y * nx;
+    const T* P = reinterpret_cast<const T*>(F.pop);
+    float d[19];
+    bool fast = true;
+    if (PARITY == 1) fast = __all_sync(__activemask(), (y - 1u < ny - 2u) && (z - 1u < nz - 2u));
+    if (PARITY == 0) {
+#pragma unroll
+        for (int q = 0; q < 19; q++) d[q] = IO::raw(sb + q * PL + li);
+    } else if (fast) {
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
+            const T* sq = sb + q * PL + li + shift[q];
+            if (cx == 0) {
+                d[q] = IO::raw(sq);
+            } else {
+                // x walls (bounce: own slot q) or x wraps (periodic x) read global memory
+                const bool edge = (cx > 0) ? (x == 0) : (x == nx - 1);
+                if (edge) {
+                    const unsigned nbr = i - (unsigned)(cx + cy * (int)nx + cz * (int)nxy);
+                    d[q] = IO::raw(P + (PERX ? qopp(q) * S + nbr + (unsigned)(cx * (int)nx) : q * S + i));
+                } else {
+                    d[q] = IO::raw(sq);
+                }
+            }
+        }
+    } else {
+        int mo[3], po[3];
+        bool mw[3], pw[3], mr[3], pr[3];
+        const unsigned c[3] = {x, y, z}, n[3] = {nx, ny, nz}, st[3] = {1u, nx, nxy};
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            mw[k] = pw[k] = mr[k] = pr[k] = false;
+            mo[k] = -(int)st[k];
+            po[k] = (int)st[k];
+            if (c[k] == 0) {
+                if (F.per[k]) {
+                    mo[k] = (int)((n[k] - 1) * st[k]);
+                    mr[k] = true;
+                } else {
+                    mw[k] = true;
+                }
+            }
+            if (c[k] == n[k] - 1) {
+                if (F.per[k]) {
+                    po[k] = -(int)((n[k] - 1) * st[k]);
+                    pr[k] = true;
+                } else {
+                    pw[k] = true;
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
+            const bool wall = (cx > 0 && mw[0]) || (cx < 0 && pw[0]) || (cy > 0 && mw[1]) || (cy < 0 && pw[1]) ||
+                              (cz > 0 && mw[2]) || (cz < 0 && pw[2]);
+            const bool wrap = (cx > 0 && mr[0]) || (cx < 0 && pr[0]) || (cy > 0 && mr[1]) || (cy < 0 && pr[1]) ||
+                              (cz > 0 && mr[2]) || (cz < 0 && pr[2]);
+            if (wall) {
+                d[q] = IO::raw(P + (q * S + i));
+            } else if (wrap) {
+                const int off = (cx > 0 ? mo[0] : cx < 0 ? po[0] : 0) + (cy > 0 ? mo[1] : cy < 0 ? po[1] : 0) +
+                                (cz > 0 ? mo[2] : cz < 0 ? po[2] : 0);
+                d[q] = IO::raw(P + (qopp(q) * S + i + (unsigned)off));
+            } else {
+                d[q] = IO::raw(sb + q * PL + li + shift[q]);
+            }
+        }
+    }
+    collide_scatter<ST, PARITY, PERX>(a, i, x, y, z, fast, false, inb, d);
+}
+
+// bounded wait for a staged tile; on time-out the error flag is set and the
+// (invalid) tile is computed anyway, so that no copy is left in flight
+__device__ __forceinline__ void wait_stage(const StepArgs& a, unsigned long long* bar, unsigned parity) {
+    unsigned spins = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (++spins > (1u << 22)) {
+            atomicOr(&a.ctl->error, kErrStageWait);
+            break;
+        }
+    }
+}
+
+template <int ST, int PARITY, int PERX>
+__global__ void __launch_bounds__(kTile, Stage<ST>::CTAS) lbm_substep_staged_kernel(StepArgs a) {
+    using T = typename Stage<ST>::T;
+    extern __shared__ __align__(128) unsigned char dsmem[];
+    // staged tile buffers 0 and 1
+    auto buf = [&](int b) { return reinterpret_cast<T*>(dsmem + (b ? Stage<ST>::BUF : 0)); };
+    __shared__ TileSlot s_slot[2];
+    __shared__ int s_shift[2][19];
+    __shared__ __align__(8) unsigned long long s_bar[2];
+    const unsigned total = (unsigned)a.n_ibm + (unsigned)a.n_tiles;
+    const unsigned n_ibm = (unsigned)a.n_ibm;
+    const bool warp0 = threadIdx.x < 32;
+    unsigned next = 0;  // thread 0: the ticket after the prepared one
+    if (threadIdx.x == 0) {
+        mbar_init(&s_bar[0], 1);
+        mbar_init(&s_bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (warp0) {
+        unsigned t0 = 0;
+        if (threadIdx.x == 0) {
+            t0 = atomicAdd(&a.tickets[a.k], 1u);
+            next = atomicAdd(&a.tickets[a.k], 1u);
+            if (t0 >= n_ibm && t0 < total) issue_tile_loads<ST, PARITY>(a, t0 - n_ibm, buf(0), s_shift[0], &s_bar[0]);
+        }
+        t0 = __shfl_sync(0xffffffffu, t0, 0);
+        prepare_slot(a, t0, s_slot[0]);
+    }
+    __syncthreads();
+    unsigned phase = 0;  // bit j: the parity of s_bar[j]'s current phase
+    for (int j = 0;; j ^= 1) {
+        const unsigned t = s_slot[j].t;
+        if (t >= total) break;
+        if (warp0) {
+            unsigned tn = 0;
+            if (threadIdx.x == 0) {
+                tn = next;
+                next = atomicAdd(&a.tickets[a.k], 1u);
+                // the other buffer was last read before the previous barrier
+                if (tn >= n_ibm && tn < total)
+                    issue_tile_loads<ST, PARITY>(a, tn - n_ibm, buf(j ^ 1), s_shift[j ^ 1], &s_bar[j ^ 1]);
+            }
+            tn = __shfl_sync(0xffffffffu, tn, 0);
+            prepare_slot(a, tn, s_slot[j ^ 1]);
+        }
+        if (t < n_ibm) {
+            ibm_task(a, t);
+        } else {
+            const TileSlot& sl = s_slot[j];
+            const int nb = sl.nb;
+            if (nb > 0) wait_ibm(a);
+            wait_stage(a, &s_bar[j], (phase >> j) & 1u);
+            phase ^= 1u << j;
+            const FluidDev& F = a.F;
+            const unsigned c0 = (t - n_ibm) * kTileCells;
+            const unsigned c1 = min(c0 + kTileCells - 1, (unsigned)F.N - 1);
+#pragma unroll 1
+            for (int r = 0; r < kCellsPerThread; r++) {
+                const unsigned li = r * kTile + threadIdx.x;
+                const unsigned i = c0 + li;
+                if (i <= c1) {
+                    bool inb = false;
+                    if (nb > 0) {
+                        const unsigned z = fdiv(i, a.div_nxy);
+                        const unsigned rem = i - z * (F.nx * F.ny);
+                        const unsigned y = fdiv(rem, a.div_nx);
+                        const unsigned x = rem - y * F.nx;
+                        for (int q = 0; q < nb; q++) inb |= inside(sl.b[q], (int)x, (int)y, (int)z);
+                    }
+                    lbm_cell_staged<ST, PARITY, PERX>(a, i, li, inb, buf(j), s_shift[j]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int ST, int PARITY, int PERX>
+static int staged_ctas_and_attr() {
+    auto k = lbm_substep_staged_kernel<ST, PARITY, PERX>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * Stage<ST>::BUF));
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTile, 2 * Stage<ST>::BUF);
+    return max(1, sms * max(1, per_sm));
+}
+
+// dynamic shared memory attributes of every staged instance; returns the
+// resident CTAs of the FP32 and the 16-bit kernels
+void staged_setup(int* ctas32, int* ctas16) {
+    *ctas32 = staged_ctas_and_attr<kStoreF32, 0, 0>();
+    staged_ctas_and_attr<kStoreF32, 1, 0>();
+    staged_ctas_and_attr<kStoreF32, 1, 1>();
+    *ctas16 = staged_ctas_and_attr<kStoreF16, 0, 0>();
+    staged_ctas_and_attr<kStoreF16, 1, 0>();
+    staged_ctas_and_attr<kStoreF16, 1, 1>();
+    staged_ctas_and_attr<kStoreBF16, 0, 0>();
+    staged_ctas_and_attr<kStoreBF16, 1, 0>();
+    staged_ctas_and_attr<kStoreBF16, 1, 1>();
 }
 
 // ---------------------------------------------------------------------------
@@ -824,6 +1168,25 @@ int lbm_resident_ctas() {
 }
 
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
+    if (a.staged_ctas > 0) {
+        const int total = a.n_ibm + a.n_tiles;
+        const dim3 g(min(total, a.staged_ctas)), b(kTile);
+#define GLSM_STAGED(ST)                                                                          \
+    if (parity && a.F.per[0])                                                                    \
+        lbm_substep_staged_kernel<ST, 1, 1><<<g, b, 2 * Stage<ST>::BUF, s>>>(a);                 \
+    else if (parity)                                                                             \
+        lbm_substep_staged_kernel<ST, 1, 0><<<g, b, 2 * Stage<ST>::BUF, s>>>(a);                 \
+    else                                                                                         \
+        lbm_substep_staged_kernel<ST, 0, 0><<<g, b, 2 * Stage<ST>::BUF, s>>>(a);
+        switch (a.F.storage) {
+            case kStoreF32: GLSM_STAGED(kStoreF32); break;
+            case kStoreF16: GLSM_STAGED(kStoreF16); break;
+            case kStoreBF16: GLSM_STAGED(kStoreBF16); break;
+            default: return cudaErrorInvalidValue;
+        }
+#undef GLSM_STAGED
+        return cudaGetLastError();
+    }
     dim3 grid(lbm_grid(a)), block(kTile);
 #define GLSM_SUB(ST)                                                           \
     if (parity && a.F.per[0])                                                  \

@@ -17,8 +17,9 @@ struct StepArgs {
     int k;               // substep index within the iteration
     int last;            // k == nsub - 1: write u for every cell
     FastDiv div_nx, div_nxy;
-    int n_tiles;         // lattice tiles of kTile cells
+    int n_tiles;         // lattice tiles of kTileCells cells
     int lbm_ctas;        // persistent CTAs per launch (0: one per ticket)
+    int staged_ctas;     // > 0: the shared-memory staged kernel with this many CTAs
 };
 
 struct ConcArgs {
@@ -55,6 +56,7 @@ cudaError_t launch_conv_diff_batch(const BatchSys* sys, const int* block_offsets
 cudaError_t launch_batch_advance(const BatchSys* sys, int n, cudaStream_t s);
 int batch_resident_ctas();
 int lbm_resident_ctas();
+void staged_setup(int* ctas32, int* ctas16);
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s);
 cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s);
 cudaError_t launch_read_pop(const FluidDev& F, int natural, float* out, cudaStream_t s);
