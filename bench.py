@@ -27,10 +27,45 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-DIMS = (101, 101, 101)
-NSUB = 25
-GELS = [((6, 6, 6), (16.67, 25.0, 25.0)), ((6, 6, 6), (33.33, 25.0, 25.0))]
 SEED, AMP = 12345, 1e-3
+
+
+def _rods():
+    """6 x 6 rods of 4x4x12 elements on a 32-unit pitch (the x/y period of the
+    384x384 lattice), standing on the z = 0 wall, anchored below z = 1.5 and
+    quiescent until a seeded delay uniform in [0, 49150) (as in
+    src/sim_array.cpp:42-51, which fires each gel's pulse at its delay)."""
+    import random
+
+    rng = random.Random(SEED)
+    gels = []
+    for iy in range(6):
+        for ix in range(6):
+            gels.append(dict(size=(4, 4, 12), pos=(16.0 + 32.0 * ix, 16.0 + 32.0 * iy, 7.5), anchor=1.5,
+                             delay=int(rng.random() * 49150)))
+    return gels
+
+
+# the measured workloads; "D" (the reference's default configuration) is the headline
+WORKLOADS = {
+    "D": dict(dims=(101, 101, 101), nsub=25, periodic=(0, 0, 0),
+              gels=[dict(size=(6, 6, 6), pos=(16.67, 25.0, 25.0)), dict(size=(6, 6, 6), pos=(33.33, 25.0, 25.0))],
+              desc="101^3 D3Q19 lattice, two 6x6x6-element gels as in sim.cpp, Nsub=25, coupled step "
+                   "(gel mechanics+BZ chemistry, IBM, LBM, concentration)"),
+    "S": dict(dims=(48, 48, 48), nsub=2, periodic=(0, 0, 0),
+              gels=[dict(size=(6, 6, 6), pos=(11.75, 11.75, 11.75))],
+              desc="48^3 D3Q19 lattice, one centred 6x6x6-element gel, Nsub=2, coupled step"),
+    "P": dict(dims=(256, 256, 256), nsub=25, periodic=(0, 0, 0),
+              gels=[dict(size=(6, 6, 6), pos=(63.75 + dx, 63.75 + dy, 63.75 + dz))
+                    for dz in (-10.0, 10.0) for dy in (-10.0, 10.0) for dx in (-10.0, 10.0)],
+              desc="256^3 D3Q19 lattice, eight 6x6x6-element gels in a 2x2x2 block 40 cells apart, Nsub=25, "
+                   "coupled step"),
+    "L": dict(dims=(384, 384, 192), nsub=3, periodic=(1, 1, 0), gels=_rods(),
+              desc="384x384x192 D3Q19 lattice periodic in x and y, 36 anchored 4x4x12-element rods on the "
+                   "z = 0 wall with seeded activation delays, Nsub=3, coupled step"),
+}
+W = WORKLOADS["D"]
+DIMS, NSUB = W["dims"], W["nsub"]
 BYTES_PER_CELL = {"f32": 152, "f16": 76, "bf16": 76}  # one read + one write of 19 populations
 FLUSH_BYTES = 256 << 20  # > the 126 MB L2
 
@@ -42,20 +77,45 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    p.add_argument("--workload", default="D", choices=sorted(WORKLOADS),
+                   help="D: 101^3 two gels (default); S: 48^3 one gel; P: 256^3 eight gels; L: 384x384x192 rods")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
     return p.parse_args()
 
 
+def select(name):
+    """Make `name` the workload of this run."""
+    global W, DIMS, NSUB
+    W = WORKLOADS[name]
+    DIMS, NSUB = W["dims"], W["nsub"]
+
+
 def workload_desc(storage):
     return {
-        "workload": "101^3 D3Q19 lattice, two 6x6x6-element gels as in sim.cpp, Nsub=25, coupled step "
-                    "(gel mechanics+BZ chemistry, IBM, LBM, concentration)",
-        "lattice": list(DIMS), "gels": len(GELS), "gel_elements": [6, 6, 6], "nsub": NSUB,
-        "storage": storage, "parallelism": "replicas (one independent system per GPU)",
+        "workload": W["desc"], "lattice": list(DIMS), "gels": len(W["gels"]),
+        "gel_elements": sorted({tuple(g["size"]) for g in W["gels"]}), "nsub": NSUB,
+        "periodic": list(W["periodic"]), "storage": storage,
+        "parallelism": "replicas (one independent system per GPU)",
         "l2": "256 MiB buffer written between timed steps",
     }
+
+
+def configure(sim):
+    """Gels, seeded chemistry noise, anchors and activation delays of the workload."""
+    for k, g in enumerate(W["gels"]):
+        sim.add_gel(g["size"], g["pos"], 1, k + 1)
+    for k, g in enumerate(W["gels"]):
+        sim.gel_noise(k, SEED, AMP)
+        if "anchor" in g:
+            sim.set_anchor(k, g["anchor"])
+        if g.get("delay", 0) > 0:
+            sim.reset_quiescent(k)
+            sim.set_active_from(k, g["delay"])
+    sim.set_params(beta=1.0, ramp_steps=20000.0, periodic=W["periodic"])
+    sim.finalize()
+    return sim
 
 
 def peaks():
@@ -68,8 +128,9 @@ def peaks():
 
 
 def ncu_traffic(storage):
-    """DRAM bytes per substep launch from the committed ncu summary, if present."""
-    path = os.path.join(ROOT, "profiles", f"lbm_substep_{storage}_101.txt")
+    """DRAM bytes per substep launch from the committed ncu summary of this
+    workload and storage, if present."""
+    path = os.path.join(ROOT, "profiles", f"lbm_substep_{storage}_{DIMS[0]}.txt")
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_launch:"):
@@ -146,12 +207,7 @@ def dist_setup(args):
 def make_system(storage):
     from glsm_fluid_3d_b200 import System
 
-    s = System(*DIMS, nsub=NSUB, storage=storage)
-    for k, (size, pos) in enumerate(GELS):
-        s.add_gel(size, pos, 1, k + 1)
-        s.gel_noise(k, SEED, AMP)
-    s.finalize()
-    return s
+    return configure(System(*DIMS, nsub=NSUB, storage=storage))
 
 
 def cpu_baseline(budget_s):
@@ -159,11 +215,7 @@ def cpu_baseline(budget_s):
     from oracle import pyoracle
 
     cores = pyoracle.threads(os.cpu_count() or 1)
-    o = pyoracle.Oracle(*DIMS, nsub=NSUB)
-    for k, (size, pos) in enumerate(GELS):
-        o.add_gel(size, pos, 1, k + 1)
-        o.gel_noise(k, SEED, AMP)
-    o.finalize()
+    o = configure(pyoracle.Oracle(*DIMS, nsub=NSUB))
     o.run(0, 1)  # warm-up
     n, t0 = 0, time.perf_counter()
     while n < 20:
@@ -175,7 +227,7 @@ def cpu_baseline(budget_s):
     o.close()
     cells = DIMS[0] * DIMS[1] * DIMS[2]
     return {"value": round(cells * NSUB * n / dt / 1e6, 3), "unit": "MLUPS", "cores": cores, "kind": "port",
-            "sample": f"{n} coupled iterations of the same 101^3 two-gel workload after 1 warm-up, FP64 oracle "
+            "sample": f"{n} coupled iterations of the same workload after 1 warm-up, FP64 oracle "
                       f"(oracle/glsm_oracle.cpp, OpenMP), {dt:.1f} s"}
 
 
@@ -336,9 +388,14 @@ def run_reference(args, world, rank, local):
                                                                 "(the reference sources were absent at build time)"}))
         return
     torch.cuda.set_device(local)
+    if any(W["periodic"]):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no periodic boundaries "
+                                                                "(this workload's x/y periodicity is an extension)"}))
+        return
     r = pyref.Reference(*DIMS, nsub=NSUB)
-    for k, (size, pos) in enumerate(GELS):
-        r.add_gel(size, pos, 1, k + 1)
+    for k, g in enumerate(W["gels"]):
+        r.add_gel(g["size"], g["pos"], 1, k + 1)
+    for k, g in enumerate(W["gels"]):
         r.gel_noise(k, SEED, AMP)
     r.set_params(beta=1.0, ramp_steps=20000.0)
     r.finalize()
@@ -379,6 +436,7 @@ def run_reference(args, world, rank, local):
 
 def main():
     args = parse()
+    select(args.workload)
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, world, rank, local)

@@ -9,10 +9,16 @@
 
 namespace glsm {
 
-constexpr int kTile = 256;        // threads of an LBM CTA
-constexpr int kCellsPerThread = 2;
+#ifndef GLSM_LBM_THREADS
+#define GLSM_LBM_THREADS 256
+#endif
+#ifndef GLSM_LBM_CELLS_PER_THREAD
+#define GLSM_LBM_CELLS_PER_THREAD 2
+#endif
+constexpr int kTile = GLSM_LBM_THREADS;  // threads of an LBM CTA
+constexpr int kCellsPerThread = GLSM_LBM_CELLS_PER_THREAD;
 constexpr int kTileCells = kTile * kCellsPerThread;  // lattice cells per LBM ticket
-constexpr int kMarkersPerTask = 8;  // IBM task CTA: one warp per marker
+constexpr int kMarkersPerTask = kTile / 32;  // IBM task CTA: one warp per marker
 constexpr int kMaxBoxes = 64;     // force-region boxes (one per gel) seen by one LBM launch
 constexpr int kGelThreads = 512;  // threads of the one-CTA-per-gel kernel
 

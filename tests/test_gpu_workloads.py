@@ -1,0 +1,100 @@
+"""The measured workloads on the GPU.
+
+* The small workload (48^3, one centred 6^3 gel, Nsub = 2) over 1,000 coupled
+  iterations against the FP64 oracle: the long-horizon counterpart of the
+  golden cases.
+* A reduced rod array with the large workload's features (x/y periodic
+  lattice, anchored rods on the z = 0 wall, staggered activation, Nsub = 3)
+  against the oracle.
+* The 256^3 eight-gel and 384x384x192 rod-array workloads build and step, and
+  stay finite and bounded.
+
+Errors are relative L2 norms; gel displacement is rn - rn(0).
+"""
+import numpy as np
+import pytest
+
+import bench
+from oracle import pyoracle
+from parity import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _fields(sim, n_gels, rn0):
+    out = {"u": sim.get(2), "c1": sim.get(3)}
+    for g in range(n_gels):
+        out[f"g{g}_disp"] = sim.get(20, g) - rn0[g]
+        out[f"g{g}_um"] = sim.get(24, g)
+        out[f"g{g}_vm"] = sim.get(25, g)
+    return out
+
+
+def _run_both(workload, iters, dims=None, gels=None, periodic=None, nsub=None):
+    from glsm_fluid_3d_b200 import System
+
+    bench.select(workload)
+    saved = dict(bench.W)
+    try:
+        if dims is not None:
+            bench.W = dict(bench.W, dims=dims, gels=gels, periodic=periodic, nsub=nsub)
+            bench.DIMS, bench.NSUB = dims, nsub
+        res = []
+        for make in (lambda: System(*bench.DIMS, nsub=bench.NSUB), lambda: pyoracle.Oracle(*bench.DIMS, nsub=bench.NSUB)):
+            sim = bench.configure(make())
+            n = len(bench.W["gels"])
+            rn0 = [sim.get(20, g) for g in range(n)]
+            sim.run(0, iters)
+            res.append(_fields(sim, n, rn0))
+            sim.close()
+        return res
+    finally:
+        bench.W = saved
+        bench.DIMS, bench.NSUB = saved["dims"], saved["nsub"]
+
+
+# CUDA (FP32 fluid, FP64 gel) vs FP64 oracle after 1,000 iterations (about ten
+# times the errors seen on B200: u 1.8e-6, c1 2.3e-7, gel fields 1e-14)
+TOL_LONG = {"u": 2e-5, "c1": 3e-6, "disp": 1e-10, "um": 1e-10, "vm": 1e-10}
+
+
+def test_small_workload_1000_iterations_vs_oracle(gpu):
+    got, want = _run_both("S", 1000)
+    bad = []
+    for k in want:
+        e = rel_l2(got[k], want[k])
+        t = TOL_LONG[k.split("_")[-1]]
+        print(f"S/1000 {k:10s} rel_l2={e:.2e} tol={t:.0e}")
+        if not e <= t:
+            bad.append((k, e, t))
+    assert not bad, bad
+
+
+def test_periodic_rod_array_vs_oracle(gpu):
+    rods = [dict(size=(2, 2, 8), pos=(4.0 + 8.0 * ix, 4.0 + 8.0 * iy, 5.5), anchor=1.5, delay=d)
+            for (ix, iy), d in zip([(0, 0), (1, 0), (0, 1), (1, 1)], [0, 3, 7, 12])]
+    got, want = _run_both("L", 20, dims=(32, 32, 24), gels=rods, periodic=(1, 1, 0), nsub=3)
+    bad = []
+    for k in want:
+        e = rel_l2(got[k], want[k])
+        t = {"u": 2e-5, "c1": 5e-6}.get(k, 1e-10)
+        print(f"rods/20 {k:10s} rel_l2={e:.2e} tol={t:.0e}")
+        if not e <= t:
+            bad.append((k, e, t))
+    assert not bad, bad
+
+
+@pytest.mark.parametrize("workload,storage", [("P", "f16"), ("P", "bf16"), ("L", "f32"), ("L", "f16")])
+def test_large_workloads_step(gpu, workload, storage):
+    bench.select(workload)
+    try:
+        s = bench.make_system(storage)
+        s.run(0, 3)
+        u = s.get(2)
+        assert np.isfinite(u).all()
+        assert np.abs(u).max() < 0.1
+        for g in range(len(bench.W["gels"])):
+            assert np.isfinite(s.get(20, g)).all()
+        s.close()
+    finally:
+        bench.select("D")
