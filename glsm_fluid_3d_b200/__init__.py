@@ -21,6 +21,7 @@ All compute runs in hand-written sm_100a kernels; there is no CPU path.
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -240,6 +241,26 @@ class Fluid:
     def run(self, iter0, n):
         """n fused, graph-captured coupled iterations starting at iter0 (asynchronous)."""
         check(self.L.glsm_fluid_run(self.h, int(iter0), int(n)), "run")
+
+    def save_checkpoint(self, path=None):
+        """Exact-restart checkpoint of the whole system (fluid, coupler, gels):
+        returned as bytes, and written to `path` when given."""
+        n = ctypes.c_size_t()
+        check(self.L.glsm_checkpoint_bytes(self.h, ctypes.byref(n)), "checkpoint size")
+        buf = np.empty(n.value, dtype=np.uint8)
+        check(self.L.glsm_checkpoint_save(self.h, buf.ctypes.data_as(ctypes.c_void_p), buf.nbytes), "checkpoint")
+        if path is not None:
+            buf.tofile(path)
+        return buf.tobytes()
+
+    def load_checkpoint(self, data):
+        """Restore a checkpoint (bytes, or the path of a file written by
+        save_checkpoint) into this system, built with the same lattice and gels."""
+        if isinstance(data, (str, os.PathLike)):
+            buf = np.fromfile(data, dtype=np.uint8)
+        else:
+            buf = np.frombuffer(data, dtype=np.uint8)
+        check(self.L.glsm_checkpoint_load(self.h, buf.ctypes.data_as(ctypes.c_void_p), buf.nbytes), "load checkpoint")
 
     def sync(self):
         check(self.L.glsm_fluid_sync(self.h), "sync")

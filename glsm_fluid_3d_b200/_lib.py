@@ -71,6 +71,9 @@ def lib():
         "glsm_fluid_units": [vp, P(f)],
         "glsm_fluid_profile_velocity": [vp, i, P(f)],
         "glsm_gel_set_bz_f": [vp, d],
+        "glsm_checkpoint_bytes": [vp, P(ctypes.c_size_t)],
+        "glsm_checkpoint_save": [vp, vp, ctypes.c_size_t],
+        "glsm_checkpoint_load": [vp, vp, ctypes.c_size_t],
         "glsm_batch_create": [P(vp)],
         "glsm_batch_destroy": [vp],
         "glsm_batch_add": [vp, vp, i, i],

@@ -64,6 +64,7 @@ struct glsm_coupler_s {
     GelDev* d_gels = nullptr;
     MarkerDev mk{};
     void* arena = nullptr;
+    size_t bytes = 0;
     Ctl* d_ctl = nullptr;
     Ctl* h_ctl = nullptr;  // pinned mirror for error reads
     cudaStream_t stream = nullptr, side = nullptr;
@@ -592,6 +593,7 @@ int glsm_coupler_create(const glsm_gel* gels, int n_gels, glsm_coupler* out) {
         delete c;
         return fail(GLSM_ERR_NOMEM, "coupler allocation: %s", cudaGetErrorString(e));
     }
+    c->bytes = bytes;
     Carver cv{(char*)c->arena};
     c->d_gels = cv.take<GelDev>(std::max(1, n_gels));
     MarkerDev& mk = c->mk;
@@ -1447,3 +1449,178 @@ int glsm_batch_destroy(glsm_batch b) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// exact-restart checkpoint of a coupled system
+// ---------------------------------------------------------------------------
+// Layout: CkptHeader, one CkptGel per gel, then the raw device bytes in this
+// order: the fluid's allocation (populations in their current AA layout, u,
+// IBM force, both concentration buffers, source, launch counters), the
+// coupler's marker state and control block, and per gel its data arrays and
+// its time-series ring.  Every region holds plain data (no device addresses),
+// so a checkpoint loads into any system built with the same lattice and gels.
+namespace {
+constexpr char kCkptMagic[8] = {'G', 'L', 'S', 'M', 'C', 'K', '0', '1'};
+struct CkptHeader {
+    char magic[8];
+    uint32_t n_gels, pad;
+    glsm_fluid_desc desc;
+    int32_t cur, pad2;
+    int64_t substeps;
+    uint64_t fluid_bytes, coupler_bytes;
+};
+// a gel's shape (checked on load) and the settings the API can change after
+// creation (restored on load)
+struct CkptGel {
+    int32_t LX, LY, LZ, type, M, marker_off, series_cap, series_every;
+    int32_t tube_mode, use_anchor, active_from, pad;
+    float tube_cy, tube_cz, tube_ihy, tube_ihz;
+    double anchor_z, f;
+    uint64_t plain_bytes, series_doubles;
+};
+
+size_t coupler_plain_off(const glsm_coupler_s* c) { return (size_t)((char*)c->mk.lag - (char*)c->arena); }
+size_t gel_plain_bytes(const glsm_gel_s* g) { return (size_t)((char*)g->d_self - (char*)g->arena); }
+
+CkptGel gel_record(const glsm_gel_s* g) {
+    const GelDev& d = g->d;
+    CkptGel r{};
+    r.LX = d.LX;
+    r.LY = d.LY;
+    r.LZ = d.LZ;
+    r.type = d.type;
+    r.M = d.M;
+    r.marker_off = d.marker_off;
+    r.series_cap = d.series_cap;
+    r.series_every = d.series_every;
+    r.tube_mode = d.tube_mode;
+    r.use_anchor = d.use_anchor;
+    r.active_from = d.active_from;
+    r.tube_cy = d.tube_cy;
+    r.tube_cz = d.tube_cz;
+    r.tube_ihy = d.tube_ihy;
+    r.tube_ihz = d.tube_ihz;
+    r.anchor_z = d.anchor_z;
+    r.f = d.f;
+    r.plain_bytes = gel_plain_bytes(g);
+    r.series_doubles = 12 * (uint64_t)d.series_cap;
+    return r;
+}
+
+void apply_gel_settings(GelDev& d, const CkptGel& r) {
+    d.tube_mode = r.tube_mode;
+    d.tube_cy = r.tube_cy;
+    d.tube_cz = r.tube_cz;
+    d.tube_ihy = r.tube_ihy;
+    d.tube_ihz = r.tube_ihz;
+    d.use_anchor = r.use_anchor;
+    d.active_from = r.active_from;
+    d.anchor_z = r.anchor_z;
+    d.f = r.f;
+    d.series_every = r.series_every;
+}
+
+size_t ckpt_bytes(const glsm_fluid_s* f) {
+    size_t n = sizeof(CkptHeader) + f->c->gels.size() * sizeof(CkptGel) + f->bytes +
+               (f->c->bytes - coupler_plain_off(f->c));
+    for (const glsm_gel_s* g : f->c->gels) n += gel_plain_bytes(g) + 12 * (size_t)g->d.series_cap * sizeof(double);
+    return n;
+}
+}  // namespace
+
+extern "C" {
+
+int glsm_checkpoint_bytes(glsm_fluid f, size_t* bytes) {
+    if (!f || !bytes) return fail(GLSM_ERR_ARG, "null argument");
+    *bytes = ckpt_bytes(f);
+    return GLSM_OK;
+}
+
+int glsm_checkpoint_save(glsm_fluid f, void* buf, size_t bytes) {
+    if (!f || !buf) return fail(GLSM_ERR_ARG, "null argument");
+    if (f->batch) return fail(GLSM_ERR_STATE, "remove the system from its batch before a checkpoint");
+    if (bytes < ckpt_bytes(f)) return fail(GLSM_ERR_ARG, "checkpoint needs %zu bytes", ckpt_bytes(f));
+    glsm_coupler c = f->c;
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaStreamSynchronize(c->side));
+    char* p = (char*)buf;
+    CkptHeader h{};
+    std::memcpy(h.magic, kCkptMagic, sizeof h.magic);
+    h.n_gels = (uint32_t)c->gels.size();
+    h.desc = f->desc;
+    h.cur = f->cur;
+    h.substeps = f->substeps;
+    h.fluid_bytes = f->bytes;
+    h.coupler_bytes = c->bytes - coupler_plain_off(c);
+    std::memcpy(p, &h, sizeof h);
+    p += sizeof h;
+    for (const glsm_gel_s* g : c->gels) {
+        const CkptGel cg = gel_record(g);
+        std::memcpy(p, &cg, sizeof cg);
+        p += sizeof cg;
+    }
+    CK(cudaMemcpy(p, f->arena, f->bytes, cudaMemcpyDeviceToHost));
+    p += f->bytes;
+    CK(cudaMemcpy(p, (char*)c->arena + coupler_plain_off(c), h.coupler_bytes, cudaMemcpyDeviceToHost));
+    p += h.coupler_bytes;
+    for (const glsm_gel_s* g : c->gels) {
+        CK(cudaMemcpy(p, g->arena, gel_plain_bytes(g), cudaMemcpyDeviceToHost));
+        p += gel_plain_bytes(g);
+        const size_t sb = 12 * (size_t)g->d.series_cap * sizeof(double);
+        CK(cudaMemcpy(p, g->d.series, sb, cudaMemcpyDeviceToHost));
+        p += sb;
+    }
+    return GLSM_OK;
+}
+
+int glsm_checkpoint_load(glsm_fluid f, const void* buf, size_t bytes) {
+    if (!f || !buf) return fail(GLSM_ERR_ARG, "null argument");
+    if (f->batch) return fail(GLSM_ERR_STATE, "remove the system from its batch before loading a checkpoint");
+    glsm_coupler c = f->c;
+    const char* p = (const char*)buf;
+    if (bytes < sizeof(CkptHeader)) return fail(GLSM_ERR_ARG, "checkpoint truncated");
+    CkptHeader h;
+    std::memcpy(&h, p, sizeof h);
+    p += sizeof h;
+    if (std::memcmp(h.magic, kCkptMagic, sizeof h.magic) != 0) return fail(GLSM_ERR_ARG, "not a checkpoint");
+    if (h.n_gels != c->gels.size()) return fail(GLSM_ERR_ARG, "checkpoint has %u gels, system %zu", h.n_gels,
+                                                c->gels.size());
+    if (std::memcmp(&h.desc, &f->desc, sizeof h.desc) != 0)
+        return fail(GLSM_ERR_ARG, "checkpoint was written by a fluid with other parameters");
+    if (h.fluid_bytes != f->bytes || h.coupler_bytes != c->bytes - coupler_plain_off(c))
+        return fail(GLSM_ERR_ARG, "checkpoint layout does not match this system");
+    if (bytes < ckpt_bytes(f)) return fail(GLSM_ERR_ARG, "checkpoint truncated");
+    std::vector<CkptGel> cgs(h.n_gels);
+    for (uint32_t i = 0; i < h.n_gels; i++) {
+        std::memcpy(&cgs[i], p, sizeof(CkptGel));
+        p += sizeof(CkptGel);
+        const CkptGel& a = cgs[i];
+        const CkptGel b = gel_record(c->gels[i]);
+        if (a.LX != b.LX || a.LY != b.LY || a.LZ != b.LZ || a.type != b.type || a.M != b.M ||
+            a.marker_off != b.marker_off || a.series_cap != b.series_cap || a.plain_bytes != b.plain_bytes ||
+            a.series_doubles != b.series_doubles)
+            return fail(GLSM_ERR_ARG, "gel %u of the checkpoint does not match this system", i);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaStreamSynchronize(c->side));
+    CK(cudaMemcpy(f->arena, p, f->bytes, cudaMemcpyHostToDevice));
+    p += f->bytes;
+    CK(cudaMemcpy((char*)c->arena + coupler_plain_off(c), p, h.coupler_bytes, cudaMemcpyHostToDevice));
+    p += h.coupler_bytes;
+    for (uint32_t i = 0; i < h.n_gels; i++) {
+        glsm_gel_s* g = c->gels[i];
+        CK(cudaMemcpy(g->arena, p, gel_plain_bytes(g), cudaMemcpyHostToDevice));
+        p += gel_plain_bytes(g);
+        const size_t sb = 12 * (size_t)g->d.series_cap * sizeof(double);
+        CK(cudaMemcpy(g->d.series, p, sb, cudaMemcpyHostToDevice));
+        p += sb;
+        apply_gel_settings(g->d, cgs[i]);
+        if (int r = upload_gel_desc(g)) return r;
+    }
+    f->cur = h.cur;
+    f->substeps = h.substeps;
+    return GLSM_OK;
+}
+
+}  // extern "C"
+

@@ -192,6 +192,23 @@ int glsm_fluid_step_concentration(glsm_fluid f, int iter);
 int glsm_fluid_run(glsm_fluid f, int iter0, int n);
 /* wait for the system stream and report device-side error flags */
 int glsm_fluid_sync(glsm_fluid f);
+
+/* ---- Exact-restart checkpoint (extension) -------------------------------
+ * The whole coupled system reachable from f (the fluid, its coupler and its
+ * gels): populations in their current layout, u, IBM force, both
+ * concentration buffers, marker state, every gel array, the time-series ring,
+ * the iteration counter and the mutable gel settings (BZ f, anchor, activation,
+ * tube mask).  Loading it restores that state byte for byte; the run then
+ * continues as an uninterrupted one would, up to the ordering of the
+ * floating-point atomics in the spreads (which also separates two runs).
+ * The reference restarts from its .dat text files through Gel::setGoonValue
+ * (src/gel.cu:221-282) and Fluid::setGoonValue, which re-initialises the
+ * populations at rest (src/fluid.cu:57-59) and reads only u and c back.
+ * A checkpoint loads into any system built with the same fluid descriptor and
+ * the same gels (sizes, types, order); the system must not be in a batch. */
+int glsm_checkpoint_bytes(glsm_fluid f, size_t* bytes);
+int glsm_checkpoint_save(glsm_fluid f, void* buf, size_t bytes);
+int glsm_checkpoint_load(glsm_fluid f, const void* buf, size_t bytes);
 /* host copies of lattice fields (FP32, reference layout) */
 int glsm_fluid_read(glsm_fluid f, int field, float* dst, size_t count);
 /* replace populations (GLSM_FLUID_POP, absolute values), u (GLSM_FLUID_U) or c1 */
