@@ -84,7 +84,8 @@ struct glsm_fluid_s {
     int cur = 0;                 // current concentration buffer
     long long substeps = 0;      // AA parity bookkeeping
     float* scratch = nullptr;    // 19*N floats, allocated on first use
-    int lbm_ctas = 0;            // resident CTAs of the persistent substep kernel
+    int lbm_ctas = 0;            // resident CTAs of the persistent substep kernel (odd substeps)
+    int lbm_ctas_even = 0;       // the same for even substeps
     int staged_ctas = 0;         // resident CTAs of the staged substep kernel (0: not used)
     struct glsm_batch_s* batch = nullptr;  // batch this system belongs to
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -797,6 +798,7 @@ static StepArgs step_args(glsm_fluid f, int k, int iter_arg) {
     a.div_nxy = make_fastdiv((unsigned)(f->F.nx * f->F.ny));
     a.n_tiles = (int)((f->F.N + kTileCells - 1) / kTileCells);
     a.lbm_ctas = f->lbm_ctas;
+    a.lbm_ctas_even = f->lbm_ctas_even;
     a.staged_ctas = f->staged_ctas;
     return a;
 }
@@ -879,7 +881,8 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     }
     int nsub_phys;
     fluid_units(d->tau, d->h, c->g2l, c->l2g, nsub_phys);
-    f->lbm_ctas = lbm_resident_ctas();
+    f->lbm_ctas = lbm_resident_ctas(d->storage, 1);
+    f->lbm_ctas_even = lbm_resident_ctas(d->storage, 0);
     {
         static int ctas32 = -1, ctas16 = -1;  // per process (one device type)
         if (ctas32 < 0) staged_setup(&ctas32, &ctas16);

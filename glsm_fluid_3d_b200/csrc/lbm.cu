@@ -58,6 +58,50 @@ struct PopIO<kStoreBF16> {
     static __device__ __forceinline__ void st_raw(T* p, float v) { *p = __float2bfloat16_rn(v); }
 };
 
+// Two adjacent cells' populations of one direction as one vector (the even
+// cell in the low half); S and the pair's first cell are even, so the vector
+// is aligned.
+template <int ST>
+struct PairIO;
+template <>
+struct PairIO<kStoreF32> {
+    using V = float2;
+    static __device__ __forceinline__ float lo(V v) { return v.x; }
+    static __device__ __forceinline__ float hi(V v) { return v.y; }
+    static __device__ __forceinline__ V set_lo(V v, float f) { return make_float2(f, v.y); }
+    static __device__ __forceinline__ V set_hi(V v, float f) { return make_float2(v.x, f); }
+};
+template <>
+struct PairIO<kStoreF16> {
+    using V = __half2;
+    static __device__ __forceinline__ float lo(V v) { return __low2float(v); }
+    static __device__ __forceinline__ float hi(V v) { return __high2float(v); }
+    static __device__ __forceinline__ V set_lo(V v, float f) { return __halves2half2(__float2half_rn(f), __high2half(v)); }
+    static __device__ __forceinline__ V set_hi(V v, float f) { return __halves2half2(__low2half(v), __float2half_rn(f)); }
+    static __device__ __forceinline__ __half lo_raw(V v) { return __low2half(v); }
+    static __device__ __forceinline__ __half hi_raw(V v) { return __high2half(v); }
+    static __device__ __forceinline__ V make(__half a, __half b) { return __halves2half2(a, b); }
+    static __device__ __forceinline__ V set_lo_raw(V v, __half a) { return __halves2half2(a, __high2half(v)); }
+    static __device__ __forceinline__ V set_hi_raw(V v, __half b) { return __halves2half2(__low2half(v), b); }
+};
+template <>
+struct PairIO<kStoreBF16> {
+    using V = __nv_bfloat162;
+    static __device__ __forceinline__ float lo(V v) { return __low2float(v); }
+    static __device__ __forceinline__ float hi(V v) { return __high2float(v); }
+    static __device__ __forceinline__ V set_lo(V v, float f) {
+        return __halves2bfloat162(__float2bfloat16_rn(f), __high2bfloat16(v));
+    }
+    static __device__ __forceinline__ V set_hi(V v, float f) {
+        return __halves2bfloat162(__low2bfloat16(v), __float2bfloat16_rn(f));
+    }
+    static __device__ __forceinline__ __nv_bfloat16 lo_raw(V v) { return __low2bfloat16(v); }
+    static __device__ __forceinline__ __nv_bfloat16 hi_raw(V v) { return __high2bfloat16(v); }
+    static __device__ __forceinline__ V make(__nv_bfloat16 a, __nv_bfloat16 b) { return __halves2bfloat162(a, b); }
+    static __device__ __forceinline__ V set_lo_raw(V v, __nv_bfloat16 a) { return __halves2bfloat162(a, __high2bfloat16(v)); }
+    static __device__ __forceinline__ V set_hi_raw(V v, __nv_bfloat16 b) { return __halves2bfloat162(__low2bfloat16(v), b); }
+};
+
 __device__ __forceinline__ int current_iter(int iter_arg, const Ctl* ctl) {
     return iter_arg >= 0 ? iter_arg : ctl->iter;
 }
@@ -339,20 +383,12 @@ __device__ __forceinline__ void collide(float (&d)[19], float Fhx, float Fhy, fl
     collide_pair<16>(d, t);
 }
 
-// force, collision and AA-pattern scatter of one cell (shared by the register
-// and the shared-memory staged gathers)
-template <int ST, int PARITY, int PERX>
-__device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, unsigned x, unsigned y, unsigned z,
-                                                bool fast, bool xin, bool inb, float (&d)[19]) {
-    using IO = PopIO<ST>;
-    using T = typename IO::T;
+// body force (uniform F_const plus, inside the marker boxes, the IBM force,
+// which the cell consumes) and collision; returns (ux, uy, uz, rho)
+template <int ST>
+__device__ __forceinline__ float4 force_collide(const StepArgs& a, unsigned i, bool inb, float (&d)[19]) {
     const FluidDev& F = a.F;
-    const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
-    const unsigned S = (unsigned)F.S, nxy = nx * ny;
-    T* P = reinterpret_cast<T*>(F.pop);
-    const long long LS = S, Lnx = nx, Lnxy = nxy;
-    // half the body force: uniform F_const plus the IBM force inside the marker boxes
-    float Fx = 0.5f * F.Fc[0], Fy = 0.5f * F.Fc[1], Fz = 0.5f * F.Fc[2];
+    float Fx = 0.5f * F.Fc[0], Fy = 0.5f * F.Fc[1], Fz = 0.5f * F.Fc[2];  // half the force
     if (inb) {
         const float4 fi = __ldcg(&F.Fibm[i]);
         Fx = fmaf(0.5f, fi.x, Fx);
@@ -360,8 +396,30 @@ __device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, u
         Fz = fmaf(0.5f, fi.z, Fz);
         __stcg(&F.Fibm[i], make_float4(0.f, 0.f, 0.f, 0.f));
     }
-    float ux, uy, uz, rho;
-    collide<IO::kScaled>(d, Fx, Fy, Fz, F.omega, F.fpref, F.inv_scale, F.scale, ux, uy, uz, rho);
+    float4 u;
+    collide<PopIO<ST>::kScaled>(d, Fx, Fy, Fz, F.omega, F.fpref, F.inv_scale, F.scale, u.x, u.y, u.z, u.w);
+    return u;
+}
+
+// the velocity moment where the next substep's interpolation (marker boxes) or
+// the concentration step (last substep) reads it
+__device__ __forceinline__ void store_u(const StepArgs& a, unsigned i, bool inb, float4 u) {
+    if (inb || a.last) a.F.u[i] = u;
+}
+
+// force, collision and AA-pattern scatter of one cell (shared by the register
+// and the shared-memory staged gathers)
+template <int ST, int PARITY, int PERX>
+__device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, unsigned x, bool fast, bool xin,
+                                                bool inb, float (&d)[19]) {
+    using IO = PopIO<ST>;
+    using T = typename IO::T;
+    const FluidDev& F = a.F;
+    const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
+    const unsigned S = (unsigned)F.S, nxy = nx * ny;
+    T* P = reinterpret_cast<T*>(F.pop);
+    const long long LS = S, Lnx = nx, Lnxy = nxy;
+    const float4 u = force_collide<ST>(a, i, inb, d);
 
     T* Pi = P + i;
     if (PARITY == 0) {
@@ -392,6 +450,8 @@ __device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, u
             }
         }
     } else {
+        const unsigned z = fdiv(i, a.div_nxy);
+        const unsigned y = fdiv(i - z * nxy, a.div_nx);
         int mo[3], po[3];
         bool mw[3], pw[3];
         const unsigned c[3] = {x, y, z}, n[3] = {nx, ny, nz}, st[3] = {1u, nx, nxy};
@@ -419,7 +479,7 @@ __device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, u
             IO::st_raw(P + (wall ? qopp(q) * S + i : q * S + i + (unsigned)off), d[q]);
         }
     }
-    if (inb || a.last) F.u[i] = make_float4(ux, uy, uz, rho);
+    store_u(a, i, inb, u);
 }
 
 // one cell of a substep: gather (AA pattern), collide, scatter.  Addresses are a
@@ -506,7 +566,7 @@ __device__ __forceinline__ void lbm_cell(const StepArgs& a, unsigned i, bool inb
             d[q] = IO::raw(P + (wall ? q * S + i : qopp(q) * S + i + (unsigned)off));
         }
     }
-    collide_scatter<ST, PARITY, PERX>(a, i, x, y, z, fast, xin, inb, d);
+    collide_scatter<ST, PARITY, PERX>(a, i, x, fast, xin, inb, d);
 }
 
 // Per-tile state prepared by warp 0 one tile ahead: the ticket and the marker
@@ -544,27 +604,74 @@ __device__ __forceinline__ void prepare_slot(const StepArgs& a, unsigned t, Tile
     }
 }
 
-// a lattice tile of kTileCells consecutive cells, kCellsPerThread per thread
-template <int ST, int PARITY, int PERX>
+// even substep of two adjacent cells i0 (even) and i0 + 1: one vector load and
+// one vector store per direction, the pair's populations staying packed in
+// registers while each cell collides in turn
+template <int ST>
+__device__ __forceinline__ void lbm_pair_even(const StepArgs& a, unsigned i0, bool inb0, bool inb1) {
+    using PIO = PairIO<ST>;
+    using V = typename PIO::V;
+    const FluidDev& F = a.F;
+    const long long LS2 = F.S >> 1;  // vectors per plane
+    V* Pv = reinterpret_cast<V*>(F.pop) + (i0 >> 1);
+    V r[19];
+#pragma unroll
+    for (int q = 0; q < 19; q++) r[q] = Pv[q * LS2];
+    {
+        float d[19];
+#pragma unroll
+        for (int q = 0; q < 19; q++) d[q] = PIO::lo(r[q]);
+        store_u(a, i0, inb0, force_collide<ST>(a, i0, inb0, d));
+#pragma unroll
+        for (int q = 0; q < 19; q++) r[q] = PIO::set_lo(r[q], d[q]);
+    }
+    {
+        float d[19];
+#pragma unroll
+        for (int q = 0; q < 19; q++) d[q] = PIO::hi(r[q]);
+        store_u(a, i0 + 1, inb1, force_collide<ST>(a, i0 + 1, inb1, d));
+#pragma unroll
+        for (int q = 0; q < 19; q++) r[q] = PIO::set_hi(r[q], d[q]);
+    }
+    // post-collision f_q goes to the cell's own slot opp(q)
+#pragma unroll
+    for (int q = 0; q < 19; q++) Pv[qopp(q) * LS2] = r[q];
+}
+
+__device__ __forceinline__ bool in_boxes(const StepArgs& a, const TileSlot& sl, int nb, unsigned i) {
+    const FluidDev& F = a.F;
+    const unsigned z = fdiv(i, a.div_nxy);
+    const unsigned rem = i - z * (F.nx * F.ny);
+    const unsigned y = fdiv(rem, a.div_nx);
+    const unsigned x = rem - y * F.nx;
+    bool inb = false;
+    for (int j = 0; j < nb; j++) inb |= inside(sl.b[j], (int)x, (int)y, (int)z);
+    return inb;
+}
+
+// a lattice tile of kTileCells consecutive cells, kCellsPerThread per thread:
+// adjacent pairs on even substeps of FP16 storage, else cells kTile apart
+template <int ST, int PARITY, int PERX, bool PAIR = false>
 __device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const TileSlot& sl) {
     const FluidDev& F = a.F;
     const unsigned c0 = tile * kTileCells;
     const unsigned c1 = min(c0 + kTileCells - 1, (unsigned)F.N - 1);
     const int nb = sl.nb;
     if (nb > 0) wait_ibm(a);
+    if constexpr (PAIR && PARITY == 0 && ST == kStoreF16 && kCellsPerThread == 2) {
+        const unsigned i0 = c0 + 2 * threadIdx.x;
+        const bool inb0 = nb > 0 && i0 <= c1 && in_boxes(a, sl, nb, i0);
+        const bool inb1 = nb > 0 && i0 + 1 <= c1 && in_boxes(a, sl, nb, i0 + 1);
+        if (i0 + 1 <= c1) {
+            lbm_pair_even<ST>(a, i0, inb0, inb1);
+        } else if (i0 <= c1) {
+            lbm_cell<ST, PARITY, PERX>(a, i0, inb0);
+        }
+    } else {
 #pragma unroll 1
-    for (int r = 0; r < kCellsPerThread; r++) {
-        const unsigned i = c0 + r * kTile + threadIdx.x;
-        if (i <= c1) {
-            bool inb = false;
-            if (nb > 0) {
-                const unsigned z = fdiv(i, a.div_nxy);
-                const unsigned rem = i - z * (F.nx * F.ny);
-                const unsigned y = fdiv(rem, a.div_nx);
-                const unsigned x = rem - y * F.nx;
-                for (int j = 0; j < nb; j++) inb |= inside(sl.b[j], (int)x, (int)y, (int)z);
-            }
-            lbm_cell<ST, PARITY, PERX>(a, i, inb);
+        for (int r = 0; r < kCellsPerThread; r++) {
+            const unsigned i = c0 + r * kTile + threadIdx.x;
+            if (i <= c1) lbm_cell<ST, PARITY, PERX>(a, i, nb > 0 && in_boxes(a, sl, nb, i));
         }
     }
 }
@@ -576,8 +683,15 @@ __device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const
 // the wait always ends (it is also bounded).  Warp 0 fetches the next ticket
 // and prepares its tile while the CTA works on the current one, so each tile
 // costs one block barrier.
+template <int ST, int PARITY>
+constexpr int lbm_ctas_per_sm() {
+    // 64 registers (4 CTAs of 256 threads per SM); 80 (3 CTAs) for the paired
+    // even substeps of FP16 storage, whose threads hold two cells
+    return (PARITY == 0 && ST == kStoreF16) ? 768 / kTile : 1024 / kTile;
+}
+
 template <int ST, int PARITY, int PERX>
-__global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
+__global__ void __launch_bounds__(kTile, (lbm_ctas_per_sm<ST, PARITY>())) lbm_substep_kernel(StepArgs a) {
     __shared__ TileSlot s_slot[2];
     const unsigned total = (unsigned)a.n_ibm + (unsigned)a.n_tiles;
     const bool warp0 = threadIdx.x < 32;
@@ -596,7 +710,7 @@ __global__ void __launch_bounds__(kTile, 4) lbm_substep_kernel(StepArgs a) {
         if (t < (unsigned)a.n_ibm)
             ibm_task(a, t);
         else
-            lbm_tile<ST, PARITY, PERX>(a, t - a.n_ibm, s_slot[j]);
+            lbm_tile<ST, PARITY, PERX, true>(a, t - a.n_ibm, s_slot[j]);
         if (warp0) {
             tn = __shfl_sync(0xffffffffu, tn, 0);
             prepare_slot(a, tn, s_slot[j ^ 1]);
@@ -759,7 +873,7 @@ __device__ __forceinline__ void lbm_cell_staged(const StepArgs& a, unsigned i, u
             }
         }
     }
-    collide_scatter<ST, PARITY, PERX>(a, i, x, y, z, fast, false, inb, d);
+    collide_scatter<ST, PARITY, PERX>(a, i, x, fast, false, inb, d);
 }
 
 // bounded wait for a staged tile; on time-out the error flag is set and the
@@ -968,7 +1082,7 @@ __device__ __forceinline__ void batch_tile(const BatchSlot& sl) {
 // Tickets: first every system's IBM tasks, then every system's tiles, so the
 // forward-progress argument of lbm_substep_kernel carries over (a tile waits
 // only for IBM tasks of its own system, all of which have lower tickets).
-__global__ void __launch_bounds__(kTile, 3) lbm_substep_batch_kernel(BatchLaunch L) {
+__global__ void __launch_bounds__(kTile, 768 / kTile) lbm_substep_batch_kernel(BatchLaunch L) {
     __shared__ BatchSlot s_slot[2];
     const unsigned total = (unsigned)(L.ibm_offsets[L.n] + L.tile_offsets[L.n]);
     const bool warp0 = threadIdx.x < 32;
@@ -1154,16 +1268,20 @@ __global__ void write_pop_kernel(FluidDev F, const float* in) {
 // ---------------------------------------------------------------------------
 // host-side launchers
 // ---------------------------------------------------------------------------
-int lbm_grid(const StepArgs& a) {
+int lbm_grid(const StepArgs& a, int parity) {
     const int total = a.n_ibm + a.n_tiles;
-    return a.lbm_ctas > 0 ? min(total, a.lbm_ctas) : total;
+    const int ctas = parity ? a.lbm_ctas : a.lbm_ctas_even;
+    return ctas > 0 ? min(total, ctas) : total;
 }
 
-int lbm_resident_ctas() {
+int lbm_resident_ctas(int storage, int parity) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF32, 1, 0>, kTile, 0);
+    if (storage == kStoreF16 && parity == 0)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF16, 0, 0>, kTile, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF32, 1, 0>, kTile, 0);
     return max(1, sms * max(1, per_sm));
 }
 
@@ -1187,7 +1305,7 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
 #undef GLSM_STAGED
         return cudaGetLastError();
     }
-    dim3 grid(lbm_grid(a)), block(kTile);
+    dim3 grid(lbm_grid(a, parity)), block(kTile);
 #define GLSM_SUB(ST)                                                           \
     if (parity && a.F.per[0])                                                  \
         lbm_substep_kernel<ST, 1, 1><<<grid, block, 0, s>>>(a);                \

@@ -18,7 +18,8 @@ struct StepArgs {
     int last;            // k == nsub - 1: write u for every cell
     FastDiv div_nx, div_nxy;
     int n_tiles;         // lattice tiles of kTileCells cells
-    int lbm_ctas;        // persistent CTAs per launch (0: one per ticket)
+    int lbm_ctas;        // persistent CTAs per odd-substep launch (0: one per ticket)
+    int lbm_ctas_even;   // persistent CTAs per even-substep launch (0: one per ticket)
     int staged_ctas;     // > 0: the shared-memory staged kernel with this many CTAs
 };
 
@@ -50,12 +51,12 @@ struct BatchLaunch {
     int last;
 };
 
-int lbm_grid(const StepArgs& a);
+int lbm_grid(const StepArgs& a, int parity);
 cudaError_t launch_substep_batch(const BatchLaunch& L, int grid, cudaStream_t s);
 cudaError_t launch_conv_diff_batch(const BatchSys* sys, const int* block_offsets, int n, int blocks, cudaStream_t s);
 cudaError_t launch_batch_advance(const BatchSys* sys, int n, cudaStream_t s);
 int batch_resident_ctas();
-int lbm_resident_ctas();
+int lbm_resident_ctas(int storage, int parity);
 void staged_setup(int* ctas32, int* ctas16);
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s);
 cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s);
