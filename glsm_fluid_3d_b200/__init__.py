@@ -271,6 +271,13 @@ class Fluid:
         check(self.L.glsm_fluid_profile_velocity(self.h, int(it), _fptr(ms)), "profile_velocity")
         return ms
 
+    def conservation(self):
+        """(mass, px, py, pz): sum of rho and of c_q f_q over the lattice, reduced
+        in FP64 on the device."""
+        out = (ctypes.c_double * 4)()
+        check(self.L.glsm_fluid_conservation(self.h, out), "conservation")
+        return tuple(out)
+
     def units(self):
         out = (ctypes.c_float * 2)()
         check(self.L.glsm_fluid_units(self.h, out), "units")

@@ -87,6 +87,7 @@ struct glsm_fluid_s {
     int lbm_ctas = 0;            // resident CTAs of the persistent substep kernel (odd substeps)
     int lbm_ctas_even = 0;       // the same for even substeps
     int staged_ctas = 0;         // resident CTAs of the staged substep kernel (0: not used)
+    double* d_cons = nullptr;    // conservation partial sums (kConsBlocks x 4) and result (4)
     struct glsm_batch_s* batch = nullptr;  // batch this system belongs to
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
 };
@@ -851,6 +852,7 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
         cv.take<float4>(N);
         for (int i = 0; i < 3; i++) cv.take<float>(N);
         cv.take<unsigned>(2 * (size_t)d->nsub);
+        cv.take<double>(4 * (size_t)kConsBlocks + 4);
         bytes = align_up(cv.off, 256);
     }
     cudaError_t e = cudaMalloc(&f->arena, bytes);
@@ -867,6 +869,7 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     F.c[1] = cv.take<float>(N);
     F.source = cv.take<float>(N);
     f->d_sync = cv.take<unsigned>(2 * (size_t)d->nsub);
+    f->d_cons = cv.take<double>(4 * (size_t)kConsBlocks + 4);
     // rest state: zero deviations (f = w), u = 0, c = 0 (k_init, fluid_kernels.cu:84-96)
     e = cudaMemsetAsync(f->arena, 0, bytes, c->stream);
     if (e == cudaSuccess) {
@@ -1114,6 +1117,18 @@ __global__ void u_unpack_kernel(const float* in, long long N, float4* u) {
 
 static int batch_wait(glsm_fluid f);
 
+int glsm_fluid_conservation(glsm_fluid f, double out[4]) {
+    if (!f || !out) return fail(GLSM_ERR_ARG, "null argument");
+    if (int r = batch_wait(f)) return r;
+    cudaStream_t s = f->c->stream;
+    // after an odd number of substeps the last one was even: populations sit in
+    // the opposite slots
+    CK(launch_conservation(f->F, (int)(f->substeps & 1), f->d_cons, f->d_cons + 4 * kConsBlocks, s));
+    CK(cudaMemcpyAsync(out, f->d_cons + 4 * kConsBlocks, 4 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return GLSM_OK;
+}
+
 int glsm_fluid_read(glsm_fluid f, int field, float* dst, size_t count) {
     if (!f || !dst) return fail(GLSM_ERR_ARG, "null argument");
     if (int r = batch_wait(f)) return r;
@@ -1209,7 +1224,7 @@ struct glsm_batch_s {
     int *d_ibm_off = nullptr, *d_tile_off = nullptr, *d_conv_off = nullptr, *d_warp_off = nullptr,
         *d_rep_off = nullptr;
     unsigned *d_tickets = nullptr, *d_ibm_done = nullptr;
-    int n_gels = 0, warps = 0, rep_blocks = 0, conv_blocks = 0;
+    int n_gels = 0, warps = 0, rep_warps = 0, conv_blocks = 0;
     int resident = 0;
     bool dirty = true;
     cudaGraphExec_t graph = nullptr;
@@ -1261,11 +1276,11 @@ static int batch_rebuild(glsm_batch_s* b) {
         tile_off[i + 1] = tile_off[i] + a.n_tiles;
         conv_off[i + 1] = conv_off[i] + (int)((f->F.N + kTile - 1) / kTile);
         warp_off[i + 1] = warp_off[i] + c->mk.M;
-        rep_off[i + 1] = rep_off[i] + (c->mk.M + 255) / 256;
+        rep_off[i + 1] = rep_off[i] + c->mk.M;  // one warp per marker
     }
     b->n_gels = (int)hg.size();
     b->warps = warp_off[n];
-    b->rep_blocks = rep_off[n];
+    b->rep_warps = rep_off[n];
     b->conv_blocks = conv_off[n];
     size_t bytes;
     {
@@ -1332,7 +1347,7 @@ static int batch_rebuild(glsm_batch_s* b) {
     if (e == cudaSuccess) e = cudaEventRecord(b->ev_fork, st);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->ev_fork, 0);
     if (e == cudaSuccess) e = launch_conc_markers_batch(b->d_mark, b->d_dyn, b->d_warp_off, n, b->warps, b->side);
-    if (e == cudaSuccess) e = launch_repulsion_batch(b->d_rep, b->d_rep_off, n, b->rep_blocks, b->side);
+    if (e == cudaSuccess) e = launch_repulsion_batch(b->d_rep, b->d_rep_off, n, b->rep_warps, b->side);
     if (e == cudaSuccess) e = cudaEventRecord(b->ev_join, b->side);
     for (int k = 0; k < b->nsub && e == cudaSuccess; k++) {
         BatchLaunch L{b->d_sys, b->d_ibm_off, b->d_tile_off, b->d_tickets, n, k, k == b->nsub - 1};

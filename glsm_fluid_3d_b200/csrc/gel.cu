@@ -551,43 +551,39 @@ __global__ void __launch_bounds__(256) conc_markers_batch_kernel(const MarkerArg
 }
 
 // ---------------------------------------------------------------------------
-// repulsion between markers of different gels (shared-memory tiles)
+// repulsion between markers of different gels: one warp per marker, the lanes
+// striding over the other markers, then a tree reduction
 // ---------------------------------------------------------------------------
-// markers [256 b, 256 b + 256) of the system described by a
-__device__ void repulsion_block(const RepulsionArgs& a, int b, float4* s_pos, int* s_own) {
+__device__ __forceinline__ float warp_sum_f(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// marker i of the system described by a (k_gel_repulsion, src/coupling_kernels.cu:90-146)
+__device__ void repulsion_marker(const RepulsionArgs& a, int i) {
     const MarkerDev& Mk = a.Mk;
-    const int M = Mk.M;
-    const int i = b * blockDim.x + threadIdx.x;
+    const int M = Mk.M, lane = threadIdx.x & 31;
     const float rcut = 2.5f * a.gamma, rc2 = rcut * rcut, sig2 = a.gamma * a.gamma;
-    float4 pi = make_float4(0, 0, 0, 0);
-    int oi = -1;
-    if (i < M) {
-        pi = Mk.lag[i];
-        oi = Mk.owner[i];
-    }
+    const float4 pi = Mk.lag[i];
+    const int oi = Mk.owner[i];
     float fx = 0.f, fy = 0.f, fz = 0.f;
-    for (int t0 = 0; t0 < M; t0 += blockDim.x) {
-        const int j = t0 + threadIdx.x;
-        s_pos[threadIdx.x] = j < M ? Mk.lag[j] : make_float4(0, 0, 0, 0);
-        s_own[threadIdx.x] = j < M ? Mk.owner[j] : -1;
-        __syncthreads();
-        const int cnt = min((int)blockDim.x, M - t0);
-        if (i < M) {
-            for (int k = 0; k < cnt; k++) {
-                if (s_own[k] == oi) continue;
-                const float dx = pi.x - s_pos[k].x, dy = pi.y - s_pos[k].y, dz = pi.z - s_pos[k].z;
-                const float r2 = dx * dx + dy * dy + dz * dz;
-                if (r2 <= 0.0f || r2 >= rc2) continue;
-                const float inv = 1.0f / r2, sr2 = sig2 * inv, sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6;
-                const float fac = 24.0f * a.delta * (2.0f * sr12 - sr6) * inv;
-                fx += fac * dx;
-                fy += fac * dy;
-                fz += fac * dz;
-            }
-        }
-        __syncthreads();
+    for (int j = lane; j < M; j += 32) {
+        if (Mk.owner[j] == oi) continue;
+        const float4 pj = Mk.lag[j];
+        const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 <= 0.0f || r2 >= rc2) continue;
+        const float inv = 1.0f / r2, sr2 = sig2 * inv, sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6;
+        const float fac = 24.0f * a.delta * (2.0f * sr12 - sr6) * inv;
+        fx += fac * dx;
+        fy += fac * dy;
+        fz += fac * dz;
     }
-    if (i < M) {
+    fx = warp_sum_f(fx);
+    fy = warp_sum_f(fy);
+    fz = warp_sum_f(fz);
+    if (lane == 0) {
         Mk.Frep[i] = make_float4(fx, fy, fz, 0.f);
         if (a.scatter) {
             const GelDev& G = a.gels[oi];
@@ -600,24 +596,21 @@ __device__ void repulsion_block(const RepulsionArgs& a, int b, float4* s_pos, in
 }
 
 __global__ void __launch_bounds__(256) repulsion_kernel(RepulsionArgs a) {
-    __shared__ float4 s_pos[256];
-    __shared__ int s_own[256];
-    repulsion_block(a, blockIdx.x, s_pos, s_own);
+    const int i = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (i < a.Mk.M) repulsion_marker(a, i);
 }
 
-// batched: block b belongs to the system whose [first, next) block range holds it
-__global__ void __launch_bounds__(256) repulsion_batch_kernel(const RepulsionArgs* systems, const int* block_offsets,
+// batched: warp w belongs to the system whose [first, next) marker range holds it
+__global__ void __launch_bounds__(256) repulsion_batch_kernel(const RepulsionArgs* systems, const int* warp_offsets,
                                                               int n) {
-    __shared__ float4 s_pos[256];
-    __shared__ int s_own[256];
-    const int b = blockIdx.x;
+    const int w = blockIdx.x * 8 + (threadIdx.x >> 5);
+    if (n <= 0 || w >= warp_offsets[n]) return;
     int lo = 0, hi = n;
     while (hi - lo > 1) {
         const int mid = (lo + hi) / 2;
-        if (block_offsets[mid] <= b) lo = mid; else hi = mid;
+        if (warp_offsets[mid] <= w) lo = mid; else hi = mid;
     }
-    if (n > 0 && b < block_offsets[n] && !(systems[lo].dyn && systems[lo].dyn->remaining == 0))
-        repulsion_block(systems[lo], b - block_offsets[lo], s_pos, s_own);
+    if (!(systems[lo].dyn && systems[lo].dyn->remaining == 0)) repulsion_marker(systems[lo], w - warp_offsets[lo]);
 }
 
 // Coupler::scatterToGels: un_robin -= Sl and Fn_robin -= Frep at each marker's node
@@ -648,7 +641,7 @@ cudaError_t launch_conc_markers(const MarkerArgs& a, cudaStream_t s) {
 
 cudaError_t launch_repulsion(const RepulsionArgs& a, cudaStream_t s) {
     if (a.Mk.M <= 0) return cudaSuccess;
-    repulsion_kernel<<<(a.Mk.M + 255) / 256, 256, 0, s>>>(a);
+    repulsion_kernel<<<(a.Mk.M + 7) / 8, 256, 0, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -665,10 +658,10 @@ cudaError_t launch_conc_markers_batch(const MarkerArgs* pairs, const SysDyn* dyn
     return cudaGetLastError();
 }
 
-cudaError_t launch_repulsion_batch(const RepulsionArgs* systems, const int* block_offsets, int n, int blocks,
+cudaError_t launch_repulsion_batch(const RepulsionArgs* systems, const int* warp_offsets, int n, int warps,
                                    cudaStream_t s) {
-    if (blocks <= 0) return cudaSuccess;
-    repulsion_batch_kernel<<<blocks, 256, 0, s>>>(systems, block_offsets, n);
+    if (warps <= 0) return cudaSuccess;
+    repulsion_batch_kernel<<<(warps + 7) / 8, 256, 0, s>>>(systems, warp_offsets, n);
     return cudaGetLastError();
 }
 

@@ -52,7 +52,7 @@ cudaError_t launch_scatter(GelDev* gels, const MarkerDev& Mk, cudaStream_t s);
 cudaError_t launch_gel_batch(const GelArgs* entries, int n, int grid, cudaStream_t s);
 cudaError_t launch_conc_markers_batch(const MarkerArgs* pairs, const SysDyn* dyn, const int* warp_offsets, int n,
                                       int warps, cudaStream_t s);
-cudaError_t launch_repulsion_batch(const RepulsionArgs* systems, const int* block_offsets, int n, int blocks,
+cudaError_t launch_repulsion_batch(const RepulsionArgs* systems, const int* warp_offsets, int n, int warps,
                                    cudaStream_t s);
 
 }  // namespace glsm

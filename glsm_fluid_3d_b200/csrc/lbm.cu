@@ -1266,6 +1266,67 @@ __global__ void write_pop_kernel(FluidDev F, const float* in) {
 }
 
 // ---------------------------------------------------------------------------
+// global mass and momentum, reduced in FP64
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sums over every cell of the stored deviations (mass: sum rho = N + sum d)
+// and of c_q d_q (momentum: the rest weights carry none), each value widened
+// to FP64 before it is added.  Every block covers a fixed set of cells and
+// writes its four partial sums; conservation_final adds them in block order,
+// so the result does not depend on scheduling.
+template <int ST>
+__global__ void __launch_bounds__(256) conservation_kernel(FluidDev F, double* partial) {
+    using IO = PopIO<ST>;
+    const typename IO::T* P = reinterpret_cast<const typename IO::T*>(F.pop);
+    double m = 0.0, px = 0.0, py = 0.0, pz = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < F.N;
+         i += (long long)gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < 19; q++) {
+            const double v = (double)IO::raw(P + (long long)q * F.S + i);
+            m += v;
+            if (qcx(q)) px += qcx(q) * v;
+            if (qcy(q)) py += qcy(q) * v;
+            if (qcz(q)) pz += qcz(q) * v;
+        }
+    }
+    __shared__ double s[4][8];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    m = warp_sum_d(m);
+    px = warp_sum_d(px);
+    py = warp_sum_d(py);
+    pz = warp_sum_d(pz);
+    if (lane == 0) {
+        s[0][w] = m;
+        s[1][w] = px;
+        s[2][w] = py;
+        s[3][w] = pz;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double t = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) t += s[threadIdx.x][k];
+        partial[4 * blockIdx.x + threadIdx.x] = t;
+    }
+}
+
+// out = (N + inv sum d, sign inv sum c d): sign = -1 when the populations sit
+// in the opposite slots (after an even AA substep)
+__global__ void conservation_final(const double* partial, int n, double inv, double cells, double sign,
+                                   double* out) {
+    const int k = threadIdx.x;
+    if (k >= 4) return;
+    double t = 0.0;
+    for (int b = 0; b < n; b++) t += partial[4 * b + k];
+    out[k] = (k == 0) ? cells + inv * t : sign * inv * t;
+}
+
+// ---------------------------------------------------------------------------
 // host-side launchers
 // ---------------------------------------------------------------------------
 int lbm_grid(const StepArgs& a, int parity) {
@@ -1362,6 +1423,18 @@ cudaError_t launch_read_pop(const FluidDev& F, int natural, float* out, cudaStre
         case kStoreBF16: read_pop_kernel<kStoreBF16><<<grid, block, 0, s>>>(F, natural, out); break;
         default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_conservation(const FluidDev& F, int reversed, double* partial, double* out, cudaStream_t s) {
+    switch (F.storage) {
+        case kStoreF32: conservation_kernel<kStoreF32><<<kConsBlocks, 256, 0, s>>>(F, partial); break;
+        case kStoreF16: conservation_kernel<kStoreF16><<<kConsBlocks, 256, 0, s>>>(F, partial); break;
+        case kStoreBF16: conservation_kernel<kStoreBF16><<<kConsBlocks, 256, 0, s>>>(F, partial); break;
+        default: return cudaErrorInvalidValue;
+    }
+    const double inv = PopIO<kStoreF16>::kScaled && F.storage == kStoreF16 ? (double)F.inv_scale : 1.0;
+    conservation_final<<<1, 32, 0, s>>>(partial, kConsBlocks, inv, (double)F.N, reversed ? -1.0 : 1.0, out);
     return cudaGetLastError();
 }
 

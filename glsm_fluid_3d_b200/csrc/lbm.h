@@ -62,5 +62,9 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s);
 cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s);
 cudaError_t launch_read_pop(const FluidDev& F, int natural, float* out, cudaStream_t s);
 cudaError_t launch_write_pop(const FluidDev& F, const float* in, cudaStream_t s);
+// global mass and momentum in FP64 (deterministic two-pass reduction); `partial`
+// holds kConsBlocks x 4 doubles, `out` receives sum(rho), sum(c f) x, y, z
+constexpr int kConsBlocks = 296;
+cudaError_t launch_conservation(const FluidDev& F, int reversed, double* partial, double* out, cudaStream_t s);
 
 }  // namespace glsm

@@ -213,6 +213,14 @@ int glsm_checkpoint_load(glsm_fluid f, const void* buf, size_t bytes);
 int glsm_fluid_read(glsm_fluid f, int field, float* dst, size_t count);
 /* replace populations (GLSM_FLUID_POP, absolute values), u (GLSM_FLUID_U) or c1 */
 int glsm_fluid_write(glsm_fluid f, int field, const float* src, size_t count);
+/* Global mass and momentum of the lattice (extension; the reference computes
+ * neither): out[0] = sum over cells of rho, out[1..3] = sum over cells and
+ * directions of c_q f_q (the population momentum, before the half-force shift
+ * of u).  Each stored population is widened to FP64 and the sums are reduced
+ * on the device in a fixed order, so the result is deterministic.  Bounce-back
+ * walls and Guo forcing conserve the mass; with all axes periodic the momentum
+ * grows by N F_const per substep. */
+int glsm_fluid_conservation(glsm_fluid f, double out[4]);
 /* nx, ny, nz, N, nsub, storage, device bytes, substeps done */
 int glsm_fluid_info(glsm_fluid f, int64_t out[8]);
 /* Fluid::stepVelocity(iter) with a CUDA event pair around each substep launch on
