@@ -271,6 +271,13 @@ class Fluid:
         check(self.L.glsm_fluid_profile_velocity(self.h, int(it), _fptr(ms)), "profile_velocity")
         return ms
 
+    def profile_substeps(self, it):
+        """stepVelocity(it) as one captured graph of its substep launches; the
+        time (ms) of the whole graph on the system stream."""
+        out = ctypes.c_float()
+        check(self.L.glsm_fluid_profile_substeps(self.h, int(it), ctypes.byref(out)), "profile_substeps")
+        return float(out.value)
+
     def conservation(self):
         """(mass, px, py, pz): sum of rho and of c_q f_q over the lattice, reduced
         in FP64 on the device."""

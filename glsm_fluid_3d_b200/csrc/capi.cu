@@ -1085,6 +1085,42 @@ int glsm_fluid_profile_velocity(glsm_fluid f, int iter, float* ms) {
     return r;
 }
 
+// Fluid::stepVelocity as a captured graph of its nsub substep launches, timed
+// with one CUDA event pair around the graph on the system stream: the
+// substep kernel back to back as it runs inside the fused iteration
+int glsm_fluid_profile_substeps(glsm_fluid f, int iter, float* total_ms) {
+    if (!f || !total_ms || iter < 0) return fail(GLSM_ERR_ARG, "bad argument");
+    if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
+    cudaStream_t s = f->c->stream;
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    int r = enqueue_velocity(f, iter, s);
+    cudaError_t e = cudaStreamEndCapture(s, &g);
+    if (r) {
+        if (g) cudaGraphDestroy(g);
+        return r;
+    }
+    if (e != cudaSuccess) return fail(GLSM_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&ge, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return fail(GLSM_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, s);
+    if (e == cudaSuccess) e = cudaGraphLaunch(ge, s);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(total_ms, e0, e1);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaGraphExecDestroy(ge);
+    if (e != cudaSuccess) return fail(GLSM_ERR_CUDA, "profile: %s", cudaGetErrorString(e));
+    f->substeps += f->F.nsub;
+    return GLSM_OK;
+}
+
 static int ensure_scratch(glsm_fluid f) {
     if (!f->scratch) CK(cudaMalloc(&f->scratch, 19 * sizeof(float) * (size_t)f->F.N));
     return GLSM_OK;
@@ -1370,8 +1406,10 @@ static int batch_rebuild(glsm_batch_s* b) {
 int glsm_batch_create(glsm_batch* out) {
     if (!out) return fail(GLSM_ERR_ARG, "null argument");
     auto* b = new glsm_batch_s;
-    cudaError_t e = cudaStreamCreate(&b->stream);
-    if (e == cudaSuccess) e = cudaStreamCreate(&b->side);
+    // non-blocking streams: work on the legacy default stream (the synchronous
+    // copies that build new systems) does not wait for a running batch
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming);
     if (e != cudaSuccess) {

@@ -120,6 +120,8 @@ class Stats:
     cell_updates: float
     max_resident: int
     batches: int
+    build_s: float = 0.0  # host time spent building systems (overlapped with running chunks)
+    wait_s: float = 0.0   # host time blocked on running chunks
 
     def summary(self) -> dict:
         lat = sorted(self.latencies)
@@ -128,11 +130,17 @@ class Stats:
                 "aggregate_mlups": round(self.cell_updates / self.makespan / 1e6, 1),
                 "p50_latency_s": round(pct(50), 3), "p99_latency_s": round(pct(99), 3),
                 "mean_latency_s": round(statistics.mean(lat), 3) if lat else None,
-                "max_resident_systems": self.max_resident, "batch_runs": self.batches}
+                "max_resident_systems": self.max_resident, "batch_runs": self.batches,
+                "build_s": round(self.build_s, 3), "wait_s": round(self.wait_s, 3)}
 
 
 class Server:
-    """Admits requests by HBM budget and advances all resident systems together."""
+    """Admits requests by HBM budget and advances all resident systems together.
+
+    Each round launches a chunk of batched iterations and, while it runs on the
+    device, builds the systems of the requests that have arrived (as far as the
+    budget allows); after the chunk it retires finished systems (reading their
+    results) and adds the newly built ones to the batch."""
 
     def __init__(self, budget_bytes: float = 150e9, max_chunk: int = 20, keep_results: bool = False):
         self.budget = budget_bytes
@@ -143,30 +151,41 @@ class Server:
     def serve(self, requests: List[Request], clock=time.perf_counter) -> Stats:
         pending = sorted(requests, key=lambda r: r.arrival)
         active = {}  # rid -> [request, system, remaining]
+        built = []   # [request, system] built while the batch ran, not yet added
         used = 0
         batch = Batch()
         lat, max_res, runs = [], 0, 0
-        work = 0.0
+        work = build_s = wait_s = 0.0
         t0 = clock()
+
+        def admit():
+            nonlocal used, build_s
+            tb = clock()
+            while pending and pending[0].arrival <= clock() - t0 and used + device_bytes(pending[0]) <= self.budget:
+                req = pending.pop(0)
+                built.append([req, build_system(req)])
+                used += device_bytes(req)
+            build_s += clock() - tb
+
         try:
-            while pending or active:
-                now = clock() - t0
-                # admission: every arrived request that fits the budget
-                while pending and pending[0].arrival <= now and used + device_bytes(pending[0]) <= self.budget:
-                    req = pending.pop(0)
-                    s = build_system(req)
+            while pending or active or built:
+                for req, s in built:
                     batch.add(s.fluid, 0, req.steps)  # the device stops it after req.steps iterations
                     active[req.rid] = [req, s, req.steps]
-                    used += device_bytes(req)
+                built.clear()
                 max_res = max(max_res, len(active))
                 if not active:
-                    if pending:  # idle until the next arrival
+                    admit()
+                    if not built and pending:  # idle until the next arrival
                         time.sleep(max(0.0, pending[0].arrival - (clock() - t0)))
                     continue
                 # a fixed chunk: members that finish inside it idle until it ends
                 chunk = min(self.max_chunk, max(v[2] for v in active.values()))
                 batch.run(chunk)
+                admit()  # overlaps the chunk running on the device
+                tw = clock()
                 batch.sync()
+                wait_s += clock() - tw
                 runs += 1
                 done = []
                 for rid, v in active.items():
@@ -187,8 +206,10 @@ class Server:
             for v in active.values():
                 batch.remove(v[1].fluid)
                 v[1].close()
+            for _, s in built:
+                s.close()
             batch.close()
-        return Stats(lat, clock() - t0, work, max_res, runs)
+        return Stats(lat, clock() - t0, work, max_res, runs, build_s, wait_s)
 
 
 def sequential(requests: List[Request], clock=time.perf_counter, keep_results: bool = False,

@@ -227,6 +227,10 @@ int glsm_fluid_info(glsm_fluid f, int64_t out[8]);
  * the system stream; ms[k] (nsub floats) receives the duration of substep k.
  * Used to report the substep kernel's achieved bandwidth. */
 int glsm_fluid_profile_velocity(glsm_fluid f, int iter, float* ms);
+/* Fluid::stepVelocity(iter) as one captured graph of its nsub substep launches,
+ * with a single CUDA event pair around it: *total_ms is the time of the nsub
+ * launches back to back, as they run inside the fused iteration graph. */
+int glsm_fluid_profile_substeps(glsm_fluid f, int iter, float* total_ms);
 /* gel_to_lbm_vel and lbm_to_gel_vel (src/fluid.cu:221-222) */
 int glsm_fluid_units(glsm_fluid f, float out[2]);
 
