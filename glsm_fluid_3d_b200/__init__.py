@@ -204,10 +204,11 @@ class Fluid:
     `dims` are lattice cells per axis (the reference derives 2*s+1 from a
     physical size s; any size is accepted here).  Keyword overrides: nsub,
     storage ("f32" | "f16" | "bf16"), tau, beta, ramp_steps, force, periodic,
-    fp16_scale, h.
+    fp16_scale, h; deterministic=True spreads by fixed-order gathers (a run
+    repeats bit for bit) instead of float atomics.
     """
 
-    def __init__(self, dims, coupler, **kw):
+    def __init__(self, dims, coupler, deterministic=False, **kw):
         self.L = lib()
         d = FluidDesc()
         check(self.L.glsm_fluid_desc_default(ctypes.byref(d), int(dims[0]), int(dims[1]), int(dims[2])), "desc")
@@ -231,6 +232,12 @@ class Fluid:
         info = (ctypes.c_int64 * 8)()
         check(self.L.glsm_fluid_info(self.h, info), "info")
         self.nx, self.ny, self.nz, self.N, self.Nsub, self.storage, self.device_bytes, _ = (int(v) for v in info)
+        if deterministic:
+            self.set_deterministic(True)
+
+    def set_deterministic(self, on=True):
+        """Spreads as fixed-order gathers (glsm_fluid_set_deterministic)."""
+        check(self.L.glsm_fluid_set_deterministic(self.h, 1 if on else 0), "set_deterministic")
 
     def stepVelocity(self, it):
         check(self.L.glsm_fluid_step_velocity(self.h, int(it)), "stepVelocity")
@@ -362,8 +369,9 @@ class System:
     oracle and the reference harness used by the tests (add_gel, gel_noise,
     set_params, finalize, run, get with the oracle's field ids)."""
 
-    def __init__(self, nx, ny, nz, nsub=25, storage="f32", fp16_scale=None, methods=False):
+    def __init__(self, nx, ny, nz, nsub=25, storage="f32", fp16_scale=None, methods=False, deterministic=False):
         self.dims = (nx, ny, nz)
+        self.deterministic = deterministic
         self.nsub = nsub
         self.storage = storage
         self.fp16_scale = fp16_scale
@@ -401,7 +409,7 @@ class System:
     def finalize(self):
         self.coupler = Coupler(self.gels)
         self.fluid = Fluid(self.dims, self.coupler, nsub=self.nsub, storage=self.storage,
-                           fp16_scale=self.fp16_scale, **self.params)
+                           fp16_scale=self.fp16_scale, deterministic=self.deterministic, **self.params)
 
     def run(self, iter0, n):
         if not self.methods:

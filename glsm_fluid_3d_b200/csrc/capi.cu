@@ -587,6 +587,7 @@ int glsm_coupler_create(const glsm_gel* gels, int n_gels, glsm_coupler* out) {
         for (int i = 0; i < 3; i++) cv.take<float4>(std::max(1, M));
         cv.take<float>(std::max(1, M));
         cv.take<Box>(kMaxBoxes);
+        cv.take<int2>(kMaxBoxes);
         cv.take<Ctl>(1);
         bytes = align_up(cv.off, 256);
     }
@@ -614,6 +615,7 @@ int glsm_coupler_create(const glsm_gel* gels, int n_gels, glsm_coupler* out) {
     mk.phz = cv.take<float4>(std::max(1, M));
     mk.wsum = cv.take<float>(std::max(1, M));
     mk.boxes = cv.take<Box>(kMaxBoxes);
+    mk.gel_range = cv.take<int2>(kMaxBoxes);
     c->d_ctl = cv.take<Ctl>(1);
     std::vector<int> owner(M);
     int off = 0;
@@ -634,6 +636,15 @@ int glsm_coupler_create(const glsm_gel* gels, int n_gels, glsm_coupler* out) {
     if (e == cudaSuccess) e = cudaHostAlloc((void**)&c->h_ctl, sizeof(Ctl), cudaHostAllocDefault);
     if (e == cudaSuccess) e = cudaMemset(c->arena, 0, bytes);
     if (e == cudaSuccess && M) e = cudaMemcpy(mk.owner, owner.data(), M * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && n_gels) {
+        std::vector<int2> ranges(n_gels);
+        int m0 = 0;
+        for (int i = 0; i < n_gels; i++) {
+            ranges[i] = make_int2(m0, m0 + c->gels[i]->d.M);
+            m0 += c->gels[i]->d.M;
+        }
+        e = cudaMemcpy(mk.gel_range, ranges.data(), n_gels * sizeof(int2), cudaMemcpyHostToDevice);
+    }
     for (int i = 0; i < n_gels && e == cudaSuccess; i++)
         e = cudaMemcpy(c->d_gels + i, &c->gels[i]->d, sizeof(GelDev), cudaMemcpyHostToDevice);
     for (int i = 0; i < n_gels && e == cudaSuccess; i++)
@@ -916,6 +927,21 @@ int glsm_fluid_destroy(glsm_fluid f) {
     return GLSM_OK;
 }
 
+int glsm_fluid_set_deterministic(glsm_fluid f, int on) {
+    if (!f) return fail(GLSM_ERR_ARG, "null fluid");
+    if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
+    CK(cudaStreamSynchronize(f->c->stream));
+    f->F.det_spread = on ? 1 : 0;
+    // the captured iteration graphs hold the old launch arguments
+    for (auto& row : f->graph)
+        for (auto& g : row)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    return GLSM_OK;
+}
+
 int glsm_fluid_units(glsm_fluid f, float out[2]) {
     if (!f || !out) return fail(GLSM_ERR_ARG, "null argument");
     out[0] = f->c->g2l;
@@ -958,7 +984,8 @@ int glsm_fluid_step_concentration(glsm_fluid f, int iter) {
     if (!f || iter < 0) return fail(GLSM_ERR_ARG, "bad argument");
     if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
     glsm_coupler c = f->c;
-    MarkerArgs m{c->d_gels, c->mk, f->F.c[f->cur], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 0};
+    MarkerArgs m{c->d_gels, c->mk, f->F.c[f->cur], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 0,
+                 f->F.det_spread};
     CK(launch_conc_markers(m, c->stream));
     ConcArgs a{f->F, c->mk, c->d_ctl, (int)c->gels.size(), f->cur, 0, make_fastdiv((unsigned)f->F.nx),
                make_fastdiv((unsigned)(f->F.nx * f->F.ny))};
@@ -981,7 +1008,8 @@ static int enqueue_iteration(glsm_fluid f, int iter_arg, int p0, int cur) {
     // markers' concentration exchange and repulsion run beside the substeps
     CK(cudaEventRecord(c->ev_fork, s));
     CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
-    MarkerArgs m{c->d_gels, c->mk, f->F.c[cur], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 1};
+    MarkerArgs m{c->d_gels, c->mk, f->F.c[cur], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 1,
+                 f->F.det_spread};
     CK(launch_conc_markers(m, c->side));
     RepulsionArgs r{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 1};
     CK(launch_repulsion(r, c->side));
@@ -1300,7 +1328,8 @@ static int batch_rebuild(glsm_batch_s* b) {
         hd[i].cur = f->cur;
         hd[i].remaining = (int)std::min<long long>(b->remaining[i], 1 << 30);
         for (int cb = 0; cb < 2; cb++)
-            hm[2 * i + cb] = MarkerArgs{c->d_gels, c->mk, f->F.c[cb], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 1};
+            hm[2 * i + cb] = MarkerArgs{c->d_gels, c->mk, f->F.c[cb], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 1,
+                                        f->F.det_spread};
         hr[i] = RepulsionArgs{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 1, nullptr};
         const int phases = kPhElastic | kPhChem | kPhRecord | kPhGather | kPhAuto;
         for (int g = 0; g < (int)c->gels.size(); g++) {

@@ -522,7 +522,7 @@ _Pragma("unroll")
             G.un_robin[G.bIndex[l - G.marker_off]] -= (double)Sl;
         }
     }
-    if (ws == 0.f) return;
+    if (ws == 0.f || a.det) return;
     const float inv_h3 = 1.0f / (a.h * a.h * a.h);
     const float scale = inv_h3 / ws;
 _Pragma("unroll")

@@ -34,6 +34,7 @@ struct MarkerArgs {
     int nx, ny, nz;
     float h;
     int scatter;       // also do un_robin -= Sl (Coupler::scatterToGels, C2 part)
+    int det;           // leave the source spread to the advection kernel's gather
 };
 
 struct RepulsionArgs {

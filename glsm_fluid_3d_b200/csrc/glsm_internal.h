@@ -96,6 +96,7 @@ struct MarkerDev {
     float4* phz;
     float* wsum;     // sum of the clipped stencil's weights (0 when empty)
     Box* boxes;      // per gel: union of its markers' clipped stencils
+    int2* gel_range; // per gel: its markers [x, y) in these arrays
 };
 
 // The lattice.  Populations are stored as deviations d_q = f_q - w_q (times
@@ -120,6 +121,7 @@ struct FluidDev {
     float dtc, Dc, inv_dx;
     float beta, ramp_steps;
     int nsub;
+    int det_spread;  // spreads as fixed-order gathers instead of float atomics
     long long substeps_done;  // host-side bookkeeping of the AA parity
 };
 

@@ -160,18 +160,64 @@ __device__ __forceinline__ bool inside(const Box& b, int x, int y, int z) {
     return x >= b.x0 && x <= b.x1 && y >= b.y0 && y <= b.y1 && z >= b.z0 && z <= b.z1;
 }
 
-// Collect into shared memory the marker boxes that overlap this CTA's tile.
-// Returns the count (all threads).  Uses one __syncthreads().
-__device__ __forceinline__ int tile_boxes(const Box* boxes, int n_boxes, const TileExt& e, Box* s_b, int* s_nb) {
-    if (threadIdx.x < n_boxes) {
-        Box b = boxes[threadIdx.x];
-        if (b.x0 <= b.x1 && overlaps(b, e)) {
-            int s = atomicAdd(s_nb, 1);
-            s_b[s] = b;
+// Collect into shared memory, in box (gel) order, the marker boxes that overlap
+// this CTA's tile and their gel indices.  Returns the count (all threads).
+// Uses one __syncthreads().
+__device__ __forceinline__ int tile_boxes(const Box* boxes, int n_boxes, const TileExt& e, Box* s_b, int* s_g,
+                                          int* s_nb) {
+    if (threadIdx.x < 32) {
+        const unsigned lane = threadIdx.x;
+        int nb = 0;
+        for (int j0 = 0; j0 < n_boxes; j0 += 32) {
+            const int j = j0 + (int)lane;
+            Box b{1, 0, 1, 0, 1, 0};
+            bool hit = false;
+            if (j < n_boxes) {
+                b = boxes[j];
+                hit = b.x0 <= b.x1 && overlaps(b, e);
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (hit) {
+                const int k = nb + __popc(m & ((1u << lane) - 1u));
+                s_b[k] = b;
+                s_g[k] = j;
+            }
+            nb += __popc(m);
         }
+        if (lane == 0) *s_nb = nb;
     }
     __syncthreads();
     return *s_nb;
+}
+
+// Deterministic form of the spreads: the sum at cell (x, y, z) of the values of
+// gel g's markers (in marker order) whose clipped 4x4x4 stencil covers the cell,
+// each times its delta-4 weight there and 1/(h^3 sum w) -- what the atomic
+// spreads (k_ibm_spread_forces, src/fluid_kernels.cu:300-348, and
+// k_ibm_spread_concentration, :414-459) add to the cell, in a fixed order.
+// CONC: the concentration source Sl (scalar, in .x); else the IBM force Fdrag.
+template <bool CONC>
+__device__ __forceinline__ void det_gather(const MarkerDev& Mk, int g, int x, int y, int z, float inv_h3, float4& acc) {
+    const int2 r = Mk.gel_range[g];
+    for (int l = r.x; l < r.y; l++) {
+        const int4 b = __ldg(&Mk.base[l]);
+        const unsigned ax = (unsigned)(x - b.x), ay = (unsigned)(y - b.y), az = (unsigned)(z - b.z);
+        if (ax > 3u || ay > 3u || az > 3u) continue;
+        if (!(((b.w >> ax) & 1) && ((b.w >> (4 + ay)) & 1) && ((b.w >> (8 + az)) & 1))) continue;
+        const float ws = __ldg(&Mk.wsum[l]);
+        if (ws == 0.0f) continue;
+        const float w = comp4(__ldg(&Mk.phx[l]), (int)ax) * comp4(__ldg(&Mk.phy[l]), (int)ay) *
+                        comp4(__ldg(&Mk.phz[l]), (int)az);
+        const float wg = w * (inv_h3 / ws);
+        if (CONC) {
+            acc.x += __ldcg(&Mk.Sl[l]) * wg;
+        } else {
+            const float4 fd = __ldcg(&Mk.Fdrag[l]);
+            acc.x += fd.x * wg;
+            acc.y += fd.y * wg;
+            acc.z += fd.z * wg;
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -220,7 +266,7 @@ __device__ __forceinline__ void ibm_marker(const StepArgs& a, int l) {
             Mk.Ul[l] = Ul;
             Mk.Fdrag[l] = Fd;
         }
-        if (ws != 0.0f) {
+        if (ws != 0.0f && !F.det_spread) {
             const float inv_h3 = (float)(1.0 / (double)(F.h * F.h * F.h));
             const float scale = inv_h3 / ws;
 #pragma unroll
@@ -575,6 +621,7 @@ struct TileSlot {
     unsigned t;
     int nb;
     Box b[kMaxBoxes];
+    int g[kMaxBoxes];  // gel index of each box
 };
 
 __device__ __forceinline__ void prepare_slot(const StepArgs& a, unsigned t, TileSlot& sl) {
@@ -594,7 +641,10 @@ __device__ __forceinline__ void prepare_slot(const StepArgs& a, unsigned t, Tile
                 hit = b.x0 <= b.x1 && overlaps(b, ext);
             }
             const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (hit) sl.b[nb + __popc(m & ((1u << lane) - 1u))] = b;
+            if (hit) {
+                sl.b[nb + __popc(m & ((1u << lane) - 1u))] = b;
+                sl.g[nb + __popc(m & ((1u << lane) - 1u))] = j;
+            }
             nb += __popc(m);
         }
     }
@@ -638,6 +688,12 @@ __device__ __forceinline__ void lbm_pair_even(const StepArgs& a, unsigned i0, bo
     for (int q = 0; q < 19; q++) Pv[qopp(q) * LS2] = r[q];
 }
 
+// whether cell i lies in a marker box of the tile; with deterministic spreads a
+// box cell also gathers its IBM force from the markers of the boxes that hold
+// it (gel order, then marker order) into Fibm[i], where the collision reads it
+// as it reads the atomically spread force otherwise
+// (DET: the deterministic-spread instantiations of the kernels)
+template <bool DET>
 __device__ __forceinline__ bool in_boxes(const StepArgs& a, const TileSlot& sl, int nb, unsigned i) {
     const FluidDev& F = a.F;
     const unsigned z = fdiv(i, a.div_nxy);
@@ -646,12 +702,19 @@ __device__ __forceinline__ bool in_boxes(const StepArgs& a, const TileSlot& sl, 
     const unsigned x = rem - y * F.nx;
     bool inb = false;
     for (int j = 0; j < nb; j++) inb |= inside(sl.b[j], (int)x, (int)y, (int)z);
+    if (DET && inb) {
+        float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float inv_h3 = (float)(1.0 / (double)(F.h * F.h * F.h));
+        for (int j = 0; j < nb; j++)
+            if (inside(sl.b[j], (int)x, (int)y, (int)z)) det_gather<false>(a.Mk, sl.g[j], (int)x, (int)y, (int)z, inv_h3, f);
+        __stcg(&F.Fibm[i], f);
+    }
     return inb;
 }
 
 // a lattice tile of kTileCells consecutive cells, kCellsPerThread per thread:
 // adjacent pairs on even substeps of FP16 storage, else cells kTile apart
-template <int ST, int PARITY, int PERX, bool PAIR = false>
+template <int ST, int PARITY, int PERX, bool PAIR = false, bool DET = false>
 __device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const TileSlot& sl) {
     const FluidDev& F = a.F;
     const unsigned c0 = tile * kTileCells;
@@ -660,8 +723,8 @@ __device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const
     if (nb > 0) wait_ibm(a);
     if constexpr (PAIR && PARITY == 0 && ST == kStoreF16 && kCellsPerThread == 2) {
         const unsigned i0 = c0 + 2 * threadIdx.x;
-        const bool inb0 = nb > 0 && i0 <= c1 && in_boxes(a, sl, nb, i0);
-        const bool inb1 = nb > 0 && i0 + 1 <= c1 && in_boxes(a, sl, nb, i0 + 1);
+        const bool inb0 = nb > 0 && i0 <= c1 && in_boxes<DET>(a, sl, nb, i0);
+        const bool inb1 = nb > 0 && i0 + 1 <= c1 && in_boxes<DET>(a, sl, nb, i0 + 1);
         if (i0 + 1 <= c1) {
             lbm_pair_even<ST>(a, i0, inb0, inb1);
         } else if (i0 <= c1) {
@@ -671,7 +734,7 @@ __device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const
 #pragma unroll 1
         for (int r = 0; r < kCellsPerThread; r++) {
             const unsigned i = c0 + r * kTile + threadIdx.x;
-            if (i <= c1) lbm_cell<ST, PARITY, PERX>(a, i, nb > 0 && in_boxes(a, sl, nb, i));
+            if (i <= c1) lbm_cell<ST, PARITY, PERX>(a, i, nb > 0 && in_boxes<DET>(a, sl, nb, i));
         }
     }
 }
@@ -690,7 +753,7 @@ constexpr int lbm_ctas_per_sm() {
     return (PARITY == 0 && ST == kStoreF16) ? 768 / kTile : 1024 / kTile;
 }
 
-template <int ST, int PARITY, int PERX>
+template <int ST, int PARITY, int PERX, bool DET>
 __global__ void __launch_bounds__(kTile, (lbm_ctas_per_sm<ST, PARITY>())) lbm_substep_kernel(StepArgs a) {
     __shared__ TileSlot s_slot[2];
     const unsigned total = (unsigned)a.n_ibm + (unsigned)a.n_tiles;
@@ -710,7 +773,7 @@ __global__ void __launch_bounds__(kTile, (lbm_ctas_per_sm<ST, PARITY>())) lbm_su
         if (t < (unsigned)a.n_ibm)
             ibm_task(a, t);
         else
-            lbm_tile<ST, PARITY, PERX, true>(a, t - a.n_ibm, s_slot[j]);
+            lbm_tile<ST, PARITY, PERX, true, DET>(a, t - a.n_ibm, s_slot[j]);
         if (warp0) {
             tn = __shfl_sync(0xffffffffu, tn, 0);
             prepare_slot(a, tn, s_slot[j ^ 1]);
@@ -950,14 +1013,7 @@ __global__ void __launch_bounds__(kTile, Stage<ST>::CTAS) lbm_substep_staged_ker
                 const unsigned li = r * kTile + threadIdx.x;
                 const unsigned i = c0 + li;
                 if (i <= c1) {
-                    bool inb = false;
-                    if (nb > 0) {
-                        const unsigned z = fdiv(i, a.div_nxy);
-                        const unsigned rem = i - z * (F.nx * F.ny);
-                        const unsigned y = fdiv(rem, a.div_nx);
-                        const unsigned x = rem - y * F.nx;
-                        for (int q = 0; q < nb; q++) inb |= inside(sl.b[q], (int)x, (int)y, (int)z);
-                    }
+                    const bool inb = nb > 0 && (F.det_spread ? in_boxes<true>(a, sl, nb, i) : in_boxes<false>(a, sl, nb, i));
                     lbm_cell_staged<ST, PARITY, PERX>(a, i, li, inb, buf(j), s_shift[j]);
                 }
             }
@@ -1058,7 +1114,10 @@ __device__ void prepare_batch_slot(const BatchLaunch& L, unsigned t, BatchSlot& 
                     hit = b.x0 <= b.x1 && overlaps(b, ext);
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, hit);
-                if (hit) sl.ts.b[nb + __popc(m & ((1u << lane) - 1u))] = b;
+                if (hit) {
+                    sl.ts.b[nb + __popc(m & ((1u << lane) - 1u))] = b;
+                    sl.ts.g[nb + __popc(m & ((1u << lane) - 1u))] = j;
+                }
                 nb += __popc(m);
             }
         }
@@ -1069,14 +1128,14 @@ __device__ void prepare_batch_slot(const BatchLaunch& L, unsigned t, BatchSlot& 
     }
 }
 
-template <int ST>
+template <int ST, bool DET>
 __device__ __forceinline__ void batch_tile(const BatchSlot& sl) {
     if (!sl.parity)
-        lbm_tile<ST, 0, 0>(sl.a, sl.local, sl.ts);
+        lbm_tile<ST, 0, 0, false, DET>(sl.a, sl.local, sl.ts);
     else if (sl.a.F.per[0])
-        lbm_tile<ST, 1, 1>(sl.a, sl.local, sl.ts);
+        lbm_tile<ST, 1, 1, false, DET>(sl.a, sl.local, sl.ts);
     else
-        lbm_tile<ST, 1, 0>(sl.a, sl.local, sl.ts);
+        lbm_tile<ST, 1, 0, false, DET>(sl.a, sl.local, sl.ts);
 }
 
 // Tickets: first every system's IBM tasks, then every system's tiles, so the
@@ -1104,12 +1163,15 @@ __global__ void __launch_bounds__(kTile, 768 / kTile) lbm_substep_batch_kernel(B
             ibm_task(sl.a, sl.local);
         } else {
             const int st = sl.a.F.storage;
-            if (st == kStoreF32)
-                batch_tile<kStoreF32>(sl);
-            else if (st == kStoreF16)
-                batch_tile<kStoreF16>(sl);
-            else
-                batch_tile<kStoreBF16>(sl);
+            if (sl.a.F.det_spread) {
+                if (st == kStoreF32) batch_tile<kStoreF32, true>(sl);
+                else if (st == kStoreF16) batch_tile<kStoreF16, true>(sl);
+                else batch_tile<kStoreBF16, true>(sl);
+            } else {
+                if (st == kStoreF32) batch_tile<kStoreF32, false>(sl);
+                else if (st == kStoreF16) batch_tile<kStoreF16, false>(sl);
+                else batch_tile<kStoreBF16, false>(sl);
+            }
         }
         if (warp0) {
             tn = __shfl_sync(0xffffffffu, tn, 0);
@@ -1123,20 +1185,16 @@ __global__ void __launch_bounds__(kTile, 768 / kTile) lbm_substep_batch_kernel(B
 // upwind advection + diffusion of the concentration (once per iteration)
 // ---------------------------------------------------------------------------
 // one 256-cell tile of the upwind advection + diffusion
-__device__ void conv_diff_tile(const ConcArgs& a, unsigned block, Box* s_b, int* s_nb_p) {
-    int& s_nb = *s_nb_p;
-    if (threadIdx.x == 0) {
-        s_nb = 0;
-        if (a.bump_iter && block == 0) a.ctl->iter += 1;  // nothing in this kernel reads it
-    }
-    __syncthreads();
+template <bool DET>
+__device__ void conv_diff_tile(const ConcArgs& a, unsigned block, Box* s_b, int* s_g, int* s_nb_p) {
+    if (threadIdx.x == 0 && a.bump_iter && block == 0) a.ctl->iter += 1;  // nothing in this kernel reads it
     const FluidDev& F = a.F;
     const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
     const unsigned N = (unsigned)F.N, nxy = nx * ny;
     const unsigned c0 = block * kTile;
     const unsigned c1 = min(c0 + kTile - 1, N - 1);
     const TileExt ext = tile_extent(c0, c1, nx, ny, a.div_nx, a.div_nxy);
-    const int nb = tile_boxes(a.Mk.boxes, a.n_boxes, ext, s_b, &s_nb);
+    const int nb = tile_boxes(a.Mk.boxes, a.n_boxes, ext, s_b, s_g, s_nb_p);
     const unsigned i = c0 + threadIdx.x;
     if (i > c1) return;
     const unsigned z = fdiv(i, a.div_nxy);
@@ -1172,17 +1230,26 @@ __device__ void conv_diff_tile(const ConcArgs& a, unsigned block, Box* s_b, int*
     const float conv = -((uR * cRx - uL * cLx) * ih + (vR * cRy - vL * cLy) * ih + (wR * cRz - wL * cLz) * ih);
     const float diff = F.Dc * ((cxm - 2.0f * c + cxp) * ih2 + (cym - 2.0f * c + cyp) * ih2 + (czm - 2.0f * c + czp) * ih2);
     float src = 0.f;
-    if (inb) {
+    if (DET && inb) {
+        // deterministic spreads: the markers' concentration source, gathered
+        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float inv_h3 = 1.0f / (F.h * F.h * F.h);
+        for (int j = 0; j < nb; j++)
+            if (inside(s_b[j], (int)x, (int)y, (int)z)) det_gather<true>(a.Mk, s_g[j], (int)x, (int)y, (int)z, inv_h3, acc);
+        src = acc.x;
+    } else if (inb) {
         src = __ldcg(&F.source[i]);
         __stcg(&F.source[i], 0.f);
     }
     c2p[i] = c + F.dtc * (conv + diff + src);
 }
 
+template <bool DET>
 __global__ void __launch_bounds__(kTile) conv_diff_kernel(ConcArgs a) {
     __shared__ int s_nb;
     __shared__ Box s_b[kMaxBoxes];
-    conv_diff_tile(a, blockIdx.x, s_b, &s_nb);
+    __shared__ int s_g[kMaxBoxes];
+    conv_diff_tile<DET>(a, blockIdx.x, s_b, s_g, &s_nb);
 }
 
 __device__ __forceinline__ int find_system(const int* offsets, int n, unsigned t) {
@@ -1199,13 +1266,17 @@ __device__ __forceinline__ int find_system(const int* offsets, int n, unsigned t
 __global__ void __launch_bounds__(kTile) conv_diff_batch_kernel(const BatchSys* sys, const int* block_offsets, int n) {
     __shared__ int s_nb;
     __shared__ Box s_b[kMaxBoxes];
+    __shared__ int s_g[kMaxBoxes];
     const unsigned b = blockIdx.x;
     if (n == 0 || b >= (unsigned)block_offsets[n]) return;
     const int s = find_system(block_offsets, n, b);
     if (sys[s].dyn->remaining == 0) return;
     ConcArgs a = sys[s].conc;
     a.cur = sys[s].dyn->cur;
-    conv_diff_tile(a, b - block_offsets[s], s_b, &s_nb);
+    if (a.F.det_spread)
+        conv_diff_tile<true>(a, b - block_offsets[s], s_b, s_g, &s_nb);
+    else
+        conv_diff_tile<false>(a, b - block_offsets[s], s_b, s_g, &s_nb);
 }
 
 // end of a batch iteration: advance every system's iteration, AA parity and
@@ -1340,9 +1411,9 @@ int lbm_resident_ctas(int storage, int parity) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (storage == kStoreF16 && parity == 0)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF16, 0, 0>, kTile, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF16, 0, 0, false>, kTile, 0);
     else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF32, 1, 0>, kTile, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF32, 1, 0, false>, kTile, 0);
     return max(1, sms * max(1, per_sm));
 }
 
@@ -1367,13 +1438,19 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
         return cudaGetLastError();
     }
     dim3 grid(lbm_grid(a, parity)), block(kTile);
-#define GLSM_SUB(ST)                                                           \
+#define GLSM_SUB2(ST, DET)                                                     \
     if (parity && a.F.per[0])                                                  \
-        lbm_substep_kernel<ST, 1, 1><<<grid, block, 0, s>>>(a);                \
+        lbm_substep_kernel<ST, 1, 1, DET><<<grid, block, 0, s>>>(a);           \
     else if (parity)                                                           \
-        lbm_substep_kernel<ST, 1, 0><<<grid, block, 0, s>>>(a);                \
+        lbm_substep_kernel<ST, 1, 0, DET><<<grid, block, 0, s>>>(a);           \
     else                                                                       \
-        lbm_substep_kernel<ST, 0, 0><<<grid, block, 0, s>>>(a);
+        lbm_substep_kernel<ST, 0, 0, DET><<<grid, block, 0, s>>>(a);
+#define GLSM_SUB(ST)            \
+    if (a.F.det_spread) {       \
+        GLSM_SUB2(ST, true)     \
+    } else {                    \
+        GLSM_SUB2(ST, false)    \
+    }
     switch (a.F.storage) {
         case kStoreF32: GLSM_SUB(kStoreF32); break;
         case kStoreF16: GLSM_SUB(kStoreF16); break;
@@ -1381,6 +1458,7 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
         default: return cudaErrorInvalidValue;
     }
 #undef GLSM_SUB
+#undef GLSM_SUB2
     return cudaGetLastError();
 }
 
@@ -1411,7 +1489,10 @@ int batch_resident_ctas() {
 
 cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s) {
     dim3 grid((unsigned)((a.F.N + kTile - 1) / kTile)), block(kTile);
-    conv_diff_kernel<<<grid, block, 0, s>>>(a);
+    if (a.F.det_spread)
+        conv_diff_kernel<true><<<grid, block, 0, s>>>(a);
+    else
+        conv_diff_kernel<false><<<grid, block, 0, s>>>(a);
     return cudaGetLastError();
 }
 

@@ -221,6 +221,14 @@ int glsm_fluid_write(glsm_fluid f, int field, const float* src, size_t count);
  * walls and Guo forcing conserve the mass; with all axes periodic the momentum
  * grows by N F_const per substep. */
 int glsm_fluid_conservation(glsm_fluid f, double out[4]);
+/* Deterministic spreads (extension; the reference spreads with float atomics,
+ * src/fluid_kernels.cu:300-348, :414-459): on = 1 makes every cell inside a
+ * marker box gather its IBM force and its concentration source from the
+ * markers whose stencils cover it -- gels in order, markers in order -- instead
+ * of the markers adding them with atomics, so that a run repeats bit for bit.
+ * Results differ from the atomic form only by round-off.  Cost: one pass over
+ * the box's markers per box cell and substep. */
+int glsm_fluid_set_deterministic(glsm_fluid f, int on);
 /* nx, ny, nz, N, nsub, storage, device bytes, substeps done */
 int glsm_fluid_info(glsm_fluid f, int64_t out[8]);
 /* Fluid::stepVelocity(iter) with a CUDA event pair around each substep launch on
