@@ -113,6 +113,16 @@ class Gel:
         check(self.L.glsm_gel_steady_state(self.h, out), "steady_state")
         return tuple(out)
 
+    def filament(self, max_points=None):
+        """calFilamentD: the u_norm = v_norm = 0.15 crossing points, (n, 3) array
+        in node units (glsm_gel_filament)."""
+        n = ctypes.c_size_t()
+        check(self.L.glsm_gel_filament(self.h, None, 0, ctypes.byref(n)), "filament")
+        cap = n.value if max_points is None else min(n.value, int(max_points))
+        out = np.zeros(3 * max(cap, 1), dtype=np.float64)
+        check(self.L.glsm_gel_filament(self.h, _dptr(out), cap, ctypes.byref(n)), "filament")
+        return out[:3 * cap].reshape(-1, 3)
+
     def series_config(self, every, capacity):
         check(self.L.glsm_gel_series_config(self.h, int(every), int(capacity)), "series_config")
         self._series_cap = int(capacity)

@@ -72,6 +72,7 @@ def lib():
         "glsm_fluid_profile_velocity": [vp, i, P(f)],
         "glsm_fluid_conservation": [vp, P(d)],
         "glsm_fluid_set_deterministic": [vp, i],
+        "glsm_gel_filament": [vp, P(d), ctypes.c_size_t, P(ctypes.c_size_t)],
         "glsm_fluid_profile_substeps": [vp, i, P(f)],
         "glsm_gel_set_bz_f": [vp, d],
         "glsm_checkpoint_bytes": [vp, P(ctypes.c_size_t)],

@@ -427,6 +427,34 @@ int glsm_gel_write(glsm_gel g, int field, const double* src, size_t count) {
 
 void* glsm_gel_device_ptr(glsm_gel g, int field) { return g ? gel_field(g, field).ptr : nullptr; }
 
+int glsm_gel_filament(glsm_gel g, double* xyz, size_t max_points, size_t* n_points) {
+    if (!g || !n_points || (max_points && !xyz)) return fail(GLSM_ERR_ARG, "null argument");
+    const size_t faces = (size_t)std::max(0, g->d.LX - 1) * std::max(0, g->d.LY - 1) * std::max(0, g->d.LZ - 1);
+    *n_points = 0;
+    if (faces == 0) return GLSM_OK;
+    cudaStream_t s = gel_stream(g);
+    double4* d_out = nullptr;
+    CK(cudaMalloc(&d_out, faces * sizeof(double4)));
+    std::vector<double4> h(faces);
+    cudaError_t e = launch_filament(g->d, d_out, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h.data(), d_out, faces * sizeof(double4), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d_out);
+    if (e != cudaSuccess) return fail(GLSM_ERR_CUDA, "filament: %s", cudaGetErrorString(e));
+    size_t n = 0;
+    for (const double4& p : h) {
+        if (p.x == 0.0) continue;
+        if (n < max_points) {
+            xyz[3 * n] = p.y;
+            xyz[3 * n + 1] = p.z;
+            xyz[3 * n + 2] = p.w;
+        }
+        n++;
+    }
+    *n_points = n;
+    return GLSM_OK;
+}
+
 }  // extern "C"
 
 // element-slot edit on the host: read um, vm, wm, apply fn(x, y, z, u, v, w), write back

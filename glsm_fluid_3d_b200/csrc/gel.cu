@@ -671,4 +671,69 @@ cudaError_t launch_scatter(GelDev* gels, const MarkerDev& Mk, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// filament (iso-line) diagnostic, calFilamentD (src/gel_kernels.cu:837-866)
+// ---------------------------------------------------------------------------
+// The point (xb, yb) in the unit square where the bilinear interpolants of
+// u (corners A B / C D) and of v (E F / G H) both equal viso, if there is one:
+// u - viso = a00 + a10 x + a01 y + a11 x y, likewise v; eliminating y leaves
+// c2 x^2 + c1 x + c0 = 0 (solveBilinear, src/gel_kernels.cu:165-212, with its
+// tolerance 1e-12 and its order of root trials).
+__device__ bool iso_crossing(double A, double B, double C, double D, double E, double Fv, double G, double H,
+                             double viso, double& xb, double& yb) {
+    const double eps = 1e-12;
+    const double a00 = A - viso, a10 = B - A, a01 = C - A, a11 = A - B + D - C;
+    const double b00 = E - viso, b10 = Fv - E, b01 = G - E, b11 = E - Fv + H - G;
+    const double c2 = b10 * a11 - b11 * a10;
+    const double c1 = b00 * a11 + b10 * a01 - b01 * a10 - b11 * a00;
+    const double c0 = b00 * a01 - b01 * a00;
+    double r[2];
+    int n = 0;
+    if (fabs(c2) < eps) {
+        if (fabs(c1) < eps) return false;
+        r[n++] = -c0 / c1;
+    } else {
+        const double disc = c1 * c1 - 4.0 * c2 * c0;
+        if (disc < 0.0) return false;
+        const double sq = sqrt(disc);
+        r[n++] = (-c1 + sq) / (2.0 * c2);
+        r[n++] = (-c1 - sq) / (2.0 * c2);
+    }
+    for (int i = 0; i < n; i++) {
+        const double x = r[i];
+        if (x < -eps || x > 1.0 + eps) continue;
+        const double den = a01 + a11 * x;
+        if (fabs(den) < eps) continue;
+        const double y = -(a00 + a10 * x) / den;
+        if (y < -eps || y > 1.0 + eps) continue;
+        xb = fmin(fmax(x, 0.0), 1.0);
+        yb = fmin(fmax(y, 0.0), 1.0);
+        return true;
+    }
+    return false;
+}
+
+// one thread per node face (xi, yi, zi), xi in [1, LX-1] etc.: out[face] =
+// (1, xi + xb, yi + yb, zi) where the u_norm = v_norm = 0.15 crossing lies,
+// else (0, 0, 0, 0); faces in x-fastest order
+__global__ void filament_kernel(GelDev G, double4* out) {
+    const int fx = G.LX - 1, fy = G.LY - 1, fz = G.LZ - 1;
+    const long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= (long long)fx * fy * fz) return;
+    const int xi = 1 + (int)(f % fx), yi = 1 + (int)((f / fx) % fy), zi = 1 + (int)(f / ((long long)fx * fy));
+    const int sx = G.LX + 2, sxy = (G.LX + 2) * (G.LY + 2);
+    const int n00 = xi + yi * sx + zi * sxy, n10 = n00 + 1, n01 = n00 + sx, n11 = n01 + 1;
+    double xb = 0.0, yb = 0.0;
+    const bool ok = iso_crossing(G.un_norm[n00], G.un_norm[n10], G.un_norm[n01], G.un_norm[n11], G.vn_norm[n00],
+                                 G.vn_norm[n10], G.vn_norm[n01], G.vn_norm[n11], 0.15, xb, yb);
+    out[f] = ok ? make_double4(1.0, xi + xb, yi + yb, (double)zi) : make_double4(0.0, 0.0, 0.0, 0.0);
+}
+
+cudaError_t launch_filament(const GelDev& G, double4* out, cudaStream_t s) {
+    const long long faces = (long long)(G.LX - 1) * (G.LY - 1) * (G.LZ - 1);
+    if (faces <= 0) return cudaSuccess;
+    filament_kernel<<<(unsigned)((faces + 255) / 256), 256, 0, s>>>(G, out);
+    return cudaGetLastError();
+}
+
 }  // namespace glsm

@@ -49,6 +49,8 @@ cudaError_t launch_gel(const GelArgs& a, int n_gels, cudaStream_t s);
 cudaError_t launch_conc_markers(const MarkerArgs& a, cudaStream_t s);
 cudaError_t launch_repulsion(const RepulsionArgs& a, cudaStream_t s);
 cudaError_t launch_scatter(GelDev* gels, const MarkerDev& Mk, cudaStream_t s);
+// per node face (x fastest): (1, x, y, z) of the u_norm = v_norm = 0.15 crossing, or zeros
+cudaError_t launch_filament(const GelDev& G, double4* out, cudaStream_t s);
 // batched forms over several systems (device arrays of per-system arguments)
 cudaError_t launch_gel_batch(const GelArgs* entries, int n, int grid, cudaStream_t s);
 cudaError_t launch_conc_markers_batch(const MarkerArgs* pairs, const SysDyn* dyn, const int* warp_offsets, int n,

@@ -157,6 +157,16 @@ int glsm_gel_write(glsm_gel g, int field, const double* src, size_t count);
 size_t glsm_gel_field_size(glsm_gel g, int field);
 /* device pointer of a field: the reference's public m_d* members */
 void* glsm_gel_device_ptr(glsm_gel g, int field);
+/* calFilamentD (src/gel_kernels.cu:837-866, run by Gel::recordCenter,
+ * src/gel.cu:706-713): the points where the nodal u_norm and v_norm fields both
+ * equal 0.15 on the node faces of each z layer -- (xi + xb, yi + yb, zi) in node
+ * units, one per face that holds a crossing, in x-fastest face order (the
+ * reference appends them in atomic order into a 300-slot buffer it never
+ * writes out).  As in the reference, y is solved from the u contour, so a face
+ * where u_norm does not vary along y reports no crossing.  Writes up to
+ * max_points points (3 doubles each) into xyz and the total count into
+ * *n_points. */
+int glsm_gel_filament(glsm_gel g, double* xyz, size_t max_points, size_t* n_points);
 
 /* ---- Coupler ------------------------------------------------------------ */
 /* Coupler::Coupler(std::vector<Gel*>&), src/coupling.h:16, src/coupling.cu:50-80 */

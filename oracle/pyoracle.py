@@ -166,3 +166,56 @@ class Oracle:
 
 def noise(seed, gel_id, slot, field):
     return lib().orc_noise(seed, gel_id, slot, field)
+
+
+def iso_crossing(A, B, C, D, E, F, G, H, viso=0.15, eps=1e-12):
+    """solveBilinear (src/gel_kernels.cu:165-212): the point (x, y) of the unit
+    square where the bilinear interpolants of u (corners A B / C D) and v
+    (E F / G H) both equal viso, or None."""
+    import math
+
+    a00, a10, a01, a11 = A - viso, B - A, C - A, A - B + D - C
+    b00, b10, b01, b11 = E - viso, F - E, G - E, E - F + H - G
+    c2 = b10 * a11 - b11 * a10
+    c1 = b00 * a11 + b10 * a01 - b01 * a10 - b11 * a00
+    c0 = b00 * a01 - b01 * a00
+    if abs(c2) < eps:
+        if abs(c1) < eps:
+            return None
+        roots = [-c0 / c1]
+    else:
+        disc = c1 * c1 - 4.0 * c2 * c0
+        if disc < 0.0:
+            return None
+        s = math.sqrt(disc)
+        roots = [(-c1 + s) / (2.0 * c2), (-c1 - s) / (2.0 * c2)]
+    for x in roots:
+        if x < -eps or x > 1.0 + eps:
+            continue
+        den = a01 + a11 * x
+        if abs(den) < eps:
+            continue
+        y = -(a00 + a10 * x) / den
+        if y < -eps or y > 1.0 + eps:
+            continue
+        return min(max(x, 0.0), 1.0), min(max(y, 0.0), 1.0)
+    return None
+
+
+def filament(un_norm, vn_norm, LX, LY, LZ, viso=0.15):
+    """calFilamentD (src/gel_kernels.cu:837-866): for every node face (xi, yi, zi),
+    xi in [1, LX-1], yi in [1, LY-1], zi in [1, LZ-1], the crossing of the
+    u_norm = viso and v_norm = viso contours as (xi + xb, yi + yb, zi); faces in
+    x-fastest order.  Nodal fields over (LX+2)(LY+2)(LZ+2) slots."""
+    sx, sxy = LX + 2, (LX + 2) * (LY + 2)
+    out = []
+    for zi in range(1, LZ):
+        for yi in range(1, LY):
+            for xi in range(1, LX):
+                n00 = xi + yi * sx + zi * sxy
+                n10, n01, n11 = n00 + 1, n00 + sx, n00 + sx + 1
+                r = iso_crossing(un_norm[n00], un_norm[n10], un_norm[n01], un_norm[n11],
+                                 vn_norm[n00], vn_norm[n10], vn_norm[n01], vn_norm[n11], viso)
+                if r is not None:
+                    out.append((xi + r[0], yi + r[1], float(zi)))
+    return np.array(out, dtype=np.float64).reshape(-1, 3)
