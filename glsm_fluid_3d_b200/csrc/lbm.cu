@@ -14,6 +14,7 @@
 //   k_stream_bounce               src/fluid_kernels.cu:144-165
 //   k_convection_diffusion        src/fluid_kernels.cu:177-242
 #include <cuda_bf16.h>
+#include <cstdlib>
 #include <cuda_fp16.h>
 
 #include "d3q19.cuh"
@@ -756,6 +757,10 @@ constexpr int lbm_ctas_per_sm() {
 template <int ST, int PARITY, int PERX, bool DET>
 __global__ void __launch_bounds__(kTile, (lbm_ctas_per_sm<ST, PARITY>())) lbm_substep_kernel(StepArgs a) {
     __shared__ TileSlot s_slot[2];
+    // programmatic dependent launch: the next substep's CTAs may start on the
+    // SMs this launch frees and run their prologue (ticket, marker boxes) while
+    // this launch's last tiles finish; they wait below for all of it
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const unsigned total = (unsigned)a.n_ibm + (unsigned)a.n_tiles;
     const bool warp0 = threadIdx.x < 32;
     if (warp0) {
@@ -764,6 +769,9 @@ __global__ void __launch_bounds__(kTile, (lbm_ctas_per_sm<ST, PARITY>())) lbm_su
         t0 = __shfl_sync(0xffffffffu, t0, 0);
         prepare_slot(a, t0, s_slot[0]);
     }
+    // every access to the previous substep's results (u, Fibm, populations)
+    // comes after the previous launch has completed and its writes are visible
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     __syncthreads();
     for (int j = 0;; j ^= 1) {
         const unsigned t = s_slot[j].t;
@@ -1438,13 +1446,26 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
         return cudaGetLastError();
     }
     dim3 grid(lbm_grid(a, parity)), block(kTile);
+    // launched with programmatic stream serialization (the kernel waits for its
+    // predecessor itself, griddepcontrol.wait); GLSM_NO_PDL=1 launches plainly
+    static const bool no_pdl = getenv("GLSM_NO_PDL") != nullptr;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = no_pdl ? 0 : 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
 #define GLSM_SUB2(ST, DET)                                                     \
     if (parity && a.F.per[0])                                                  \
-        lbm_substep_kernel<ST, 1, 1, DET><<<grid, block, 0, s>>>(a);           \
+        return cudaLaunchKernelEx(&cfg, lbm_substep_kernel<ST, 1, 1, DET>, a); \
     else if (parity)                                                           \
-        lbm_substep_kernel<ST, 1, 0, DET><<<grid, block, 0, s>>>(a);           \
+        return cudaLaunchKernelEx(&cfg, lbm_substep_kernel<ST, 1, 0, DET>, a); \
     else                                                                       \
-        lbm_substep_kernel<ST, 0, 0, DET><<<grid, block, 0, s>>>(a);
+        return cudaLaunchKernelEx(&cfg, lbm_substep_kernel<ST, 0, 0, DET>, a);
 #define GLSM_SUB(ST)            \
     if (a.F.det_spread) {       \
         GLSM_SUB2(ST, true)     \
