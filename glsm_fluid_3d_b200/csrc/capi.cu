@@ -750,7 +750,8 @@ int glsm_coupler_scatter(glsm_coupler c) {
 
 int glsm_coupler_repulsion(glsm_coupler c) {
     if (!c) return fail(GLSM_ERR_ARG, "null coupler");
-    RepulsionArgs r{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 0};
+    RepulsionArgs r{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 0, nullptr, (int)c->gels.size(),
+                    c->fluid ? c->fluid->F.h : 0.0f};
     CK(launch_repulsion(r, c->stream));
     return GLSM_OK;
 }
@@ -1039,7 +1040,7 @@ static int enqueue_iteration(glsm_fluid f, int iter_arg, int p0, int cur) {
     MarkerArgs m{c->d_gels, c->mk, f->F.c[cur], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 1,
                  f->F.det_spread};
     CK(launch_conc_markers(m, c->side));
-    RepulsionArgs r{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 1};
+    RepulsionArgs r{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 1, nullptr, (int)c->gels.size(), f->F.h};
     CK(launch_repulsion(r, c->side));
     CK(cudaEventRecord(c->ev_join, c->side));
     for (int k = 0; k < nsub; k++) CK(launch_substep(step_args(f, k, iter_arg), (p0 + k) & 1, s));
@@ -1358,7 +1359,7 @@ static int batch_rebuild(glsm_batch_s* b) {
         for (int cb = 0; cb < 2; cb++)
             hm[2 * i + cb] = MarkerArgs{c->d_gels, c->mk, f->F.c[cb], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 1,
                                         f->F.det_spread};
-        hr[i] = RepulsionArgs{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 1, nullptr};
+        hr[i] = RepulsionArgs{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 1, nullptr, (int)c->gels.size(), f->F.h};
         const int phases = kPhElastic | kPhChem | kPhRecord | kPhGather | kPhAuto;
         for (int g = 0; g < (int)c->gels.size(); g++) {
             GelArgs ga = coupler_gel_args(c, phases, -1);

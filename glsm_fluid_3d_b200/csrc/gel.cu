@@ -560,7 +560,23 @@ __device__ __forceinline__ float warp_sum_f(float v) {
     return v;
 }
 
-// marker i of the system described by a (k_gel_repulsion, src/coupling_kernels.cu:90-146)
+// the LJ force of marker j on marker i, added to f when within the cut-off
+__device__ __forceinline__ void lj_pair(const RepulsionArgs& a, float4 pi, float4 pj, float rc2, float sig2, float& fx,
+                                        float& fy, float& fz) {
+    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 <= 0.0f || r2 >= rc2) return;
+    const float inv = 1.0f / r2, sr2 = sig2 * inv, sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6;
+    const float fac = 24.0f * a.delta * (2.0f * sr12 - sr6) * inv;
+    fx += fac * dx;
+    fy += fac * dy;
+    fz += fac * dz;
+}
+
+// marker i of the system described by a (k_gel_repulsion, src/coupling_kernels.cu:90-146).
+// With the marker boxes known (h > 0), a gel is visited only when marker i lies
+// within the cut-off of its box (the union of its markers' stencils, which
+// holds every one of its markers): the same pairs, without the far gels' markers.
 __device__ void repulsion_marker(const RepulsionArgs& a, int i) {
     const MarkerDev& Mk = a.Mk;
     const int M = Mk.M, lane = threadIdx.x & 31;
@@ -568,17 +584,20 @@ __device__ void repulsion_marker(const RepulsionArgs& a, int i) {
     const float4 pi = Mk.lag[i];
     const int oi = Mk.owner[i];
     float fx = 0.f, fy = 0.f, fz = 0.f;
-    for (int j = lane; j < M; j += 32) {
-        if (Mk.owner[j] == oi) continue;
-        const float4 pj = Mk.lag[j];
-        const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 <= 0.0f || r2 >= rc2) continue;
-        const float inv = 1.0f / r2, sr2 = sig2 * inv, sr6 = sr2 * sr2 * sr2, sr12 = sr6 * sr6;
-        const float fac = 24.0f * a.delta * (2.0f * sr12 - sr6) * inv;
-        fx += fac * dx;
-        fy += fac * dy;
-        fz += fac * dz;
+    if (a.h > 0.0f) {
+        for (int g = 0; g < a.n_gels; g++) {
+            if (g == oi) continue;
+            const Box b = Mk.boxes[g];
+            if (b.x0 > b.x1) continue;
+            if (pi.x < b.x0 * a.h - rcut || pi.x > (b.x1 + 1) * a.h + rcut || pi.y < b.y0 * a.h - rcut ||
+                pi.y > (b.y1 + 1) * a.h + rcut || pi.z < b.z0 * a.h - rcut || pi.z > (b.z1 + 1) * a.h + rcut)
+                continue;
+            const int2 r = Mk.gel_range[g];
+            for (int j = r.x + lane; j < r.y; j += 32) lj_pair(a, pi, Mk.lag[j], rc2, sig2, fx, fy, fz);
+        }
+    } else {
+        for (int j = lane; j < M; j += 32)
+            if (Mk.owner[j] != oi) lj_pair(a, pi, Mk.lag[j], rc2, sig2, fx, fy, fz);
     }
     fx = warp_sum_f(fx);
     fy = warp_sum_f(fy);

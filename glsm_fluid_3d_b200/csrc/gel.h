@@ -43,6 +43,8 @@ struct RepulsionArgs {
     float delta, gamma;
     int scatter;       // also do Fn_robin -= Frep
     const SysDyn* dyn; // batched systems: skip when dyn->remaining == 0
+    int n_gels;        // with h > 0: skip gels whose marker box is out of reach
+    float h;           // lattice cell width (0: no marker boxes yet, every pair)
 };
 
 cudaError_t launch_gel(const GelArgs& a, int n_gels, cudaStream_t s);
