@@ -197,6 +197,24 @@ class Clocks:
                 "reasons": sorted(set().union(*[r[4] for r in inside])), "samples": len(inside)}
 
 
+def max_over_ranks(value, world, device):
+    """The job time of a replicated run: the largest of the ranks' times (every
+    rank calls this with its own; NCCL on GPUs, any backend that has MAX)."""
+    if world <= 1:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_value(cells, nsub, steps, world, t_seconds):
+    """Whole-job MLUPS of `world` replicas, each advancing `cells` x `nsub` cell
+    updates per step for `steps` steps, over the job time."""
+    return world * cells * nsub * steps / t_seconds / 1e6
+
+
 def dist_setup(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -277,13 +295,9 @@ def run_ours(args, world, rank, local):
     t_wall1 = time.time()
     clk = clocks.stop(t_wall0, t_wall1)
     fluid.sync()
-    t_ms = sum(a.elapsed_time(b) for a, b in ev)
-    if world > 1:
-        t = torch.tensor([t_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        t_ms = float(t.item())
+    t_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world, "cuda")
     N = DIMS[0] * DIMS[1] * DIMS[2]
-    value = world * N * NSUB * K / (t_ms / 1e3) / 1e6
+    value = job_value(N, NSUB, K, world, t_ms / 1e3)
 
     # dominant kernel: the substep kernel.  Each velocity step's nsub launches
     # run as one captured graph timed by an event pair on the system stream
@@ -351,12 +365,8 @@ def run_ours(args, world, rank, local):
         fluid.read_into("u", host_u)
         fluid.read_into("c1", host_c)
         barrier()
-        t_e2e = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([t_e2e], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            t_e2e = float(t.item())
-        e2e = {"value": round(world * N * NSUB * K / t_e2e / 1e6, 1), "unit": "MLUPS",
+        t_e2e = max_over_ranks(time.perf_counter() - t0, world, "cuda")
+        e2e = {"value": round(job_value(N, NSUB, K, world, t_e2e), 1), "unit": "MLUPS",
                "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": int(d2h / K),
                "timing": "host wall clock around the whole job, device synchronised at both ends",
                "job": "restart of gel chemistry/positions and u, c from pinned host memory (H2D), K fused "
