@@ -1151,6 +1151,9 @@ __device__ __forceinline__ void batch_tile(const BatchSlot& sl) {
 // only for IBM tasks of its own system, all of which have lower tickets).
 __global__ void __launch_bounds__(kTile, 768 / kTile) lbm_substep_batch_kernel(BatchLaunch L) {
     __shared__ BatchSlot s_slot[2];
+    // programmatic dependent launch as in lbm_substep_kernel (from the second
+    // substep of an iteration on)
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     const unsigned total = (unsigned)(L.ibm_offsets[L.n] + L.tile_offsets[L.n]);
     const bool warp0 = threadIdx.x < 32;
     if (warp0) {
@@ -1159,6 +1162,7 @@ __global__ void __launch_bounds__(kTile, 768 / kTile) lbm_substep_batch_kernel(B
         t0 = __shfl_sync(0xffffffffu, t0, 0);
         prepare_batch_slot(L, t0, s_slot[0]);
     }
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     __syncthreads();
     for (int j = 0;; j ^= 1) {
         const BatchSlot& sl = s_slot[j];
@@ -1446,12 +1450,15 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
         return cudaGetLastError();
     }
     dim3 grid(lbm_grid(a, parity)), block(kTile);
-    // launched with programmatic stream serialization (the kernel waits for its
-    // predecessor itself, griddepcontrol.wait); GLSM_NO_PDL=1 launches plainly
+    // substeps after the first are launched with programmatic stream
+    // serialization (the kernel waits for its predecessor itself,
+    // griddepcontrol.wait); the first follows the kernels that rewrite the
+    // marker boxes its prologue reads, so it is launched plainly.  GLSM_NO_PDL=1
+    // launches every substep plainly.
     static const bool no_pdl = getenv("GLSM_NO_PDL") != nullptr;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = no_pdl ? 0 : 1;
+    attr[0].val.programmaticStreamSerializationAllowed = (no_pdl || a.k == 0) ? 0 : 1;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
@@ -1484,8 +1491,17 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
 }
 
 cudaError_t launch_substep_batch(const BatchLaunch& L, int grid, cudaStream_t s) {
-    lbm_substep_batch_kernel<<<grid, kTile, 0, s>>>(L);
-    return cudaGetLastError();
+    static const bool no_pdl = getenv("GLSM_NO_PDL") != nullptr;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = (no_pdl || L.k == 0) ? 0 : 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kTile);
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, lbm_substep_batch_kernel, L);
 }
 
 cudaError_t launch_conv_diff_batch(const BatchSys* sys, const int* block_offsets, int n, int blocks, cudaStream_t s) {
