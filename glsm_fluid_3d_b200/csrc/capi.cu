@@ -1314,13 +1314,19 @@ struct glsm_batch_s {
     GelArgs* d_gel = nullptr;
     MarkerArgs* d_mark = nullptr;
     RepulsionArgs* d_rep = nullptr;
-    int *d_ibm_off = nullptr, *d_tile_off = nullptr, *d_conv_off = nullptr, *d_warp_off = nullptr,
-        *d_rep_off = nullptr;
+    int *d_members = nullptr, *d_ibm_off = nullptr, *d_tile_off = nullptr, *d_conv_off = nullptr,
+        *d_warp_off = nullptr, *d_rep_off = nullptr;
     unsigned *d_tickets = nullptr, *d_ibm_done = nullptr;
     int n_gels = 0, warps = 0, rep_warps = 0, conv_blocks = 0;
-    int resident = 0;
     bool dirty = true;
-    cudaGraphExec_t graph = nullptr;
+    // one iteration graph per parity phase: with an odd nsub every running
+    // system's substep parity flips from one iteration to the next
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    int phase = 0;
+    // streams on which the substep launches of groups 1.. run (group 0 runs
+    // on `stream`), and the events that join them back
+    std::vector<cudaStream_t> gstreams;
+    std::vector<cudaEvent_t> gevents;
 };
 
 static int batch_wait(glsm_fluid f) {
@@ -1329,8 +1335,11 @@ static int batch_wait(glsm_fluid f) {
 }
 
 static void batch_free_device(glsm_batch_s* b) {
-    if (b->graph) cudaGraphExecDestroy(b->graph);
-    b->graph = nullptr;
+    for (auto& g : b->graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+    b->phase = 0;
 }
 
 // device descriptors of the current members; recapture of the iteration graph
@@ -1345,7 +1354,44 @@ static int batch_rebuild(glsm_batch_s* b) {
     std::vector<GelArgs> hg;
     std::vector<MarkerArgs> hm(2 * (size_t)n);
     std::vector<RepulsionArgs> hr(n);
-    std::vector<int> ibm_off(n + 1, 0), tile_off(n + 1, 0), conv_off(n + 1, 0), warp_off(n + 1, 0), rep_off(n + 1, 0);
+    std::vector<int> conv_off(n + 1, 0), warp_off(n + 1, 0), rep_off(n + 1, 0);
+    // Groups: systems that share storage, x periodicity, spread mode and the
+    // parity of their substep count share one kernel instantiation for every
+    // substep (their parities stay equal).  Each group has its own member
+    // list, prefix sums of IBM tasks and tiles, and ticket counters.
+    struct Group {
+        BatchGroupKey key;
+        int p0;
+        std::vector<int> members;
+    };
+    std::vector<Group> groups;
+    for (int i = 0; i < n; i++) {
+        const glsm_fluid_s* f = b->sys[i];
+        const BatchGroupKey key{f->F.storage, f->F.per[0], f->F.det_spread};
+        const int p0 = (int)(f->substeps & 1);
+        auto it = std::find_if(groups.begin(), groups.end(), [&](const Group& g) {
+            return g.key.storage == key.storage && g.key.perx == key.perx && g.key.det == key.det && g.p0 == p0;
+        });
+        if (it == groups.end()) {
+            groups.push_back(Group{key, p0, {}});
+            it = groups.end() - 1;
+        }
+        it->members.push_back(i);
+    }
+    const int G = (int)groups.size();
+    std::vector<int> members, gibm_off, gtile_off, g_total(G);
+    for (int gi = 0; gi < G; gi++) {
+        int io = 0, to = 0;
+        gibm_off.push_back(0);
+        gtile_off.push_back(0);
+        for (int i : groups[gi].members) {
+            const StepArgs a = step_args(b->sys[i], 0, -1);
+            members.push_back(i);
+            gibm_off.push_back(io += a.n_ibm);
+            gtile_off.push_back(to += a.n_tiles);
+        }
+        g_total[gi] = io + to;
+    }
     for (int i = 0; i < n; i++) {
         glsm_fluid_s* f = b->sys[i];
         glsm_coupler c = f->c;
@@ -1366,8 +1412,6 @@ static int batch_rebuild(glsm_batch_s* b) {
             ga.first_gel = g;
             hg.push_back(ga);
         }
-        ibm_off[i + 1] = ibm_off[i] + a.n_ibm;
-        tile_off[i + 1] = tile_off[i] + a.n_tiles;
         conv_off[i + 1] = conv_off[i] + (int)((f->F.N + kTile - 1) / kTile);
         warp_off[i + 1] = warp_off[i] + c->mk.M;
         rep_off[i + 1] = rep_off[i] + c->mk.M;  // one warp per marker
@@ -1384,8 +1428,10 @@ static int batch_rebuild(glsm_batch_s* b) {
         cv.take<GelArgs>(std::max<size_t>(1, hg.size()));
         cv.take<MarkerArgs>(2 * (size_t)n);
         cv.take<RepulsionArgs>(n);
-        for (int k = 0; k < 5; k++) cv.take<int>(n + 1);
-        cv.take<unsigned>(b->nsub);
+        cv.take<int>(n);
+        for (int k = 0; k < 2; k++) cv.take<int>(n + G);
+        for (int k = 0; k < 3; k++) cv.take<int>(n + 1);
+        cv.take<unsigned>((size_t)G * b->nsub);
         cv.take<unsigned>((size_t)n * b->nsub);
         bytes = align_up(cv.off, 256);
     }
@@ -1402,12 +1448,13 @@ static int batch_rebuild(glsm_batch_s* b) {
     b->d_gel = cv.take<GelArgs>(std::max<size_t>(1, hg.size()));
     b->d_mark = cv.take<MarkerArgs>(2 * (size_t)n);
     b->d_rep = cv.take<RepulsionArgs>(n);
-    b->d_ibm_off = cv.take<int>(n + 1);
-    b->d_tile_off = cv.take<int>(n + 1);
+    b->d_members = cv.take<int>(n);
+    b->d_ibm_off = cv.take<int>(n + G);
+    b->d_tile_off = cv.take<int>(n + G);
     b->d_conv_off = cv.take<int>(n + 1);
     b->d_warp_off = cv.take<int>(n + 1);
     b->d_rep_off = cv.take<int>(n + 1);
-    b->d_tickets = cv.take<unsigned>(b->nsub);
+    b->d_tickets = cv.take<unsigned>((size_t)G * b->nsub);
     b->d_ibm_done = cv.take<unsigned>((size_t)n * b->nsub);
     for (int i = 0; i < n; i++) {
         hs[i].dyn = b->d_dyn + i;
@@ -1425,39 +1472,72 @@ static int batch_rebuild(glsm_batch_s* b) {
     if (!hg.empty()) CK(cudaMemcpy(b->d_gel, hg.data(), hg.size() * sizeof(GelArgs), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b->d_mark, hm.data(), hm.size() * sizeof(MarkerArgs), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b->d_rep, hr.data(), hr.size() * sizeof(RepulsionArgs), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->d_ibm_off, ibm_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(b->d_tile_off, tile_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_members, members.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_ibm_off, gibm_off.data(), (n + G) * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(b->d_tile_off, gtile_off.data(), (n + G) * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b->d_conv_off, conv_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b->d_warp_off, warp_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b->d_rep_off, rep_off.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice));
 
-    // capture one batch iteration
+    while ((int)b->gstreams.size() < G - 1) {
+        cudaStream_t gs = nullptr;
+        cudaEvent_t ge = nullptr;
+        CK(cudaStreamCreateWithFlags(&gs, cudaStreamNonBlocking));
+        b->gstreams.push_back(gs);
+        CK(cudaEventCreateWithFlags(&ge, cudaEventDisableTiming));
+        b->gevents.push_back(ge);
+    }
+    std::vector<int> resident(2 * G);
+    for (int gi = 0; gi < G; gi++)
+        for (int p = 0; p < 2; p++) resident[2 * gi + p] = batch_resident_ctas(groups[gi].key, p);
+
+    // capture one batch iteration per parity phase; the groups' substep
+    // chains run on their own streams, side by side on the GPU
     cudaStream_t st = b->stream;
-    cudaGraph_t g = nullptr;
-    CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaMemsetAsync(b->d_tickets, 0, b->nsub * sizeof(unsigned), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ibm_done, 0, (size_t)n * b->nsub * sizeof(unsigned), st);
-    if (e == cudaSuccess) e = launch_gel_batch(b->d_gel, b->n_gels, b->n_gels, st);
-    if (e == cudaSuccess) e = cudaEventRecord(b->ev_fork, st);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->ev_fork, 0);
-    if (e == cudaSuccess) e = launch_conc_markers_batch(b->d_mark, b->d_dyn, b->d_warp_off, n, b->warps, b->side);
-    if (e == cudaSuccess) e = launch_repulsion_batch(b->d_rep, b->d_rep_off, n, b->rep_warps, b->side);
-    if (e == cudaSuccess) e = cudaEventRecord(b->ev_join, b->side);
-    for (int k = 0; k < b->nsub && e == cudaSuccess; k++) {
-        BatchLaunch L{b->d_sys, b->d_ibm_off, b->d_tile_off, b->d_tickets, n, k, k == b->nsub - 1};
-        e = launch_substep_batch(L, std::min(b->resident, ibm_off[n] + tile_off[n]), st);
+    const int n_phases = (b->nsub & 1) ? 2 : 1;
+    for (int ph = 0; ph < n_phases; ph++) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaMemsetAsync(b->d_tickets, 0, (size_t)G * b->nsub * sizeof(unsigned), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(b->d_ibm_done, 0, (size_t)n * b->nsub * sizeof(unsigned), st);
+        if (e == cudaSuccess) e = launch_gel_batch(b->d_gel, b->n_gels, b->n_gels, st);
+        if (e == cudaSuccess) e = cudaEventRecord(b->ev_fork, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(b->side, b->ev_fork, 0);
+        if (e == cudaSuccess) e = launch_conc_markers_batch(b->d_mark, b->d_dyn, b->d_warp_off, n, b->warps, b->side);
+        if (e == cudaSuccess) e = launch_repulsion_batch(b->d_rep, b->d_rep_off, n, b->rep_warps, b->side);
+        if (e == cudaSuccess) e = cudaEventRecord(b->ev_join, b->side);
+        int moff = 0;
+        for (int gi = 0; gi < G && e == cudaSuccess; gi++) {
+            const Group& gr = groups[gi];
+            const int ng = (int)gr.members.size();
+            cudaStream_t gs = gi == 0 ? st : b->gstreams[gi - 1];
+            if (gi > 0) e = cudaStreamWaitEvent(gs, b->ev_fork, 0);
+            for (int k = 0; k < b->nsub && e == cudaSuccess; k++) {
+                const int parity = (gr.p0 + ph * b->nsub + k) & 1;
+                BatchLaunch L{b->d_sys, b->d_members + moff, b->d_ibm_off + moff + gi, b->d_tile_off + moff + gi,
+                              b->d_tickets + (size_t)gi * b->nsub, ng, k, k == b->nsub - 1};
+                e = launch_substep_batch(L, gr.key, parity, std::min(resident[2 * gi + parity], g_total[gi]), gs);
+            }
+            if (gi > 0 && e == cudaSuccess) e = cudaEventRecord(b->gevents[gi - 1], gs);
+            if (gi > 0 && e == cudaSuccess) e = cudaStreamWaitEvent(st, b->gevents[gi - 1], 0);
+            moff += ng;
+        }
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->ev_join, 0);
+        if (e == cudaSuccess) e = launch_conv_diff_batch(b->d_sys, b->d_conv_off, n, b->conv_blocks, st);
+        if (e == cudaSuccess) e = launch_batch_advance(b->d_sys, n, st);
+        cudaError_t e2 = cudaStreamEndCapture(st, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            b->dirty = true;
+            return fail(GLSM_ERR_CUDA, "batch capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
+        }
+        e = cudaGraphInstantiate(&b->graph[ph], g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            b->dirty = true;
+            return fail(GLSM_ERR_CUDA, "batch instantiate: %s", cudaGetErrorString(e));
+        }
     }
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, b->ev_join, 0);
-    if (e == cudaSuccess) e = launch_conv_diff_batch(b->d_sys, b->d_conv_off, n, b->conv_blocks, st);
-    if (e == cudaSuccess) e = launch_batch_advance(b->d_sys, n, st);
-    cudaError_t e2 = cudaStreamEndCapture(st, &g);
-    if (e != cudaSuccess || e2 != cudaSuccess) {
-        if (g) cudaGraphDestroy(g);
-        return fail(GLSM_ERR_CUDA, "batch capture: %s", cudaGetErrorString(e != cudaSuccess ? e : e2));
-    }
-    e = cudaGraphInstantiate(&b->graph, g, 0);
-    cudaGraphDestroy(g);
-    if (e != cudaSuccess) return fail(GLSM_ERR_CUDA, "batch instantiate: %s", cudaGetErrorString(e));
     return GLSM_OK;
 }
 
@@ -1474,7 +1554,6 @@ int glsm_batch_create(glsm_batch* out) {
         delete b;
         return fail(GLSM_ERR_CUDA, "batch: %s", cudaGetErrorString(e));
     }
-    b->resident = batch_resident_ctas();
     *out = b;
     return GLSM_OK;
 }
@@ -1515,7 +1594,10 @@ int glsm_batch_run(glsm_batch b, int n) {
         if (r) return r;
     }
     if (b->sys.empty() || n == 0) return GLSM_OK;
-    for (int it = 0; it < n; it++) CK(cudaGraphLaunch(b->graph, b->stream));
+    for (int it = 0; it < n; it++) {
+        CK(cudaGraphLaunch(b->graph[b->phase], b->stream));
+        if (b->graph[1]) b->phase ^= 1;
+    }
     for (size_t i = 0; i < b->sys.size(); i++) {
         glsm_fluid_s* f = b->sys[i];
         long long& rem = b->remaining[i];
@@ -1556,6 +1638,8 @@ int glsm_batch_destroy(glsm_batch b) {
     if (b->arena) cudaFree(b->arena);
     cudaEventDestroy(b->ev_fork);
     cudaEventDestroy(b->ev_join);
+    for (auto ge : b->gevents) cudaEventDestroy(ge);
+    for (auto gs : b->gstreams) cudaStreamDestroy(gs);
     cudaStreamDestroy(b->side);
     cudaStreamDestroy(b->stream);
     delete b;

@@ -1058,12 +1058,13 @@ void staged_setup(int* ctas32, int* ctas16) {
 // ---------------------------------------------------------------------------
 // batched substep: several systems in one persistent launch
 // ---------------------------------------------------------------------------
+// The systems of a batch are launched in groups that share storage, x
+// periodicity, spread mode and substep parity, so each group launch is the
+// single-system kernel's instantiation with a different ticket resolver.
 struct BatchSlot {
-    TileSlot ts;     // global ticket and the tile's marker boxes
-    int sys;         // system index
+    TileSlot ts;     // group ticket and the tile's marker boxes
     unsigned local;  // IBM task or tile index within the system
     int is_ibm;
-    int parity;
     int idle;        // the ticket belongs to a system that has finished
     StepArgs a;      // the system's arguments for this substep
 };
@@ -1077,7 +1078,7 @@ __device__ __forceinline__ int find_sys(const int* offsets, int n, unsigned t) {
     return lo;
 }
 
-// warp 0: resolve global ticket t to (system, local work) and prepare the slot
+// warp 0: resolve group ticket t to (system, local work) and prepare the slot
 __device__ void prepare_batch_slot(const BatchLaunch& L, unsigned t, BatchSlot& sl) {
     const unsigned lane = threadIdx.x & 31;
     const unsigned n_ibm_all = (unsigned)L.ibm_offsets[L.n];
@@ -1085,8 +1086,9 @@ __device__ void prepare_batch_slot(const BatchLaunch& L, unsigned t, BatchSlot& 
     int nb = 0;
     if (t < total) {
         const bool ibm = t < n_ibm_all;
-        const int s = ibm ? find_sys(L.ibm_offsets, L.n, t) : find_sys(L.tile_offsets, L.n, t - n_ibm_all);
-        if (L.sys[s].dyn->remaining == 0) {  // an idle system: nothing to do for this ticket
+        const int g = ibm ? find_sys(L.ibm_offsets, L.n, t) : find_sys(L.tile_offsets, L.n, t - n_ibm_all);
+        const BatchSys& sys = L.sys[L.members[g]];
+        if (sys.dyn->remaining == 0) {  // an idle system: nothing to do for this ticket
             if (lane == 0) {
                 sl.ts.t = t;
                 sl.ts.nb = 0;
@@ -1094,8 +1096,8 @@ __device__ void prepare_batch_slot(const BatchLaunch& L, unsigned t, BatchSlot& 
             }
             return;
         }
-        const unsigned local = ibm ? t - L.ibm_offsets[s] : (t - n_ibm_all) - L.tile_offsets[s];
-        const int* src = reinterpret_cast<const int*>(&L.sys[s].step);
+        const unsigned local = ibm ? t - L.ibm_offsets[g] : (t - n_ibm_all) - L.tile_offsets[g];
+        const int* src = reinterpret_cast<const int*>(&sys.step);
         int* dst = reinterpret_cast<int*>(&sl.a);
         for (int w = lane; w < (int)(sizeof(StepArgs) / 4); w += 32) dst[w] = src[w];
         __syncwarp();  // the whole copy lands before lane 0 sets the per-launch fields
@@ -1103,13 +1105,11 @@ __device__ void prepare_batch_slot(const BatchLaunch& L, unsigned t, BatchSlot& 
             sl.idle = 0;
             sl.a.k = L.k;
             sl.a.last = L.last;
-            sl.sys = s;
             sl.local = local;
             sl.is_ibm = ibm;
-            sl.parity = (L.sys[s].dyn->parity0 + L.k) & 1;
         }
         if (!ibm) {
-            const StepArgs& a = L.sys[s].step;
+            const StepArgs& a = sys.step;
             const unsigned c0 = local * kTileCells;
             const unsigned c1 = min(c0 + kTileCells - 1, (unsigned)a.F.N - 1);
             const TileExt ext = tile_extent(c0, c1, a.F.nx, a.F.ny, a.div_nx, a.div_nxy);
@@ -1136,20 +1136,21 @@ __device__ void prepare_batch_slot(const BatchLaunch& L, unsigned t, BatchSlot& 
     }
 }
 
-template <int ST, bool DET>
-__device__ __forceinline__ void batch_tile(const BatchSlot& sl) {
-    if (!sl.parity)
-        lbm_tile<ST, 0, 0, false, DET>(sl.a, sl.local, sl.ts);
-    else if (sl.a.F.per[0])
-        lbm_tile<ST, 1, 1, false, DET>(sl.a, sl.local, sl.ts);
-    else
-        lbm_tile<ST, 1, 0, false, DET>(sl.a, sl.local, sl.ts);
+// The batched tiles read the system's parameters from the shared-memory slot
+// rather than from the constant bank; on even substeps that costs registers
+// (at 64 a thread spills about 170 bytes), so the batched even substeps take
+// 80 registers (3 CTAs of 256 threads per SM) and the odd ones the
+// single-system budget.
+template <int ST, int PARITY>
+constexpr int batch_ctas_per_sm() {
+    return PARITY == 0 ? 768 / kTile : lbm_ctas_per_sm<ST, PARITY>();
 }
 
-// Tickets: first every system's IBM tasks, then every system's tiles, so the
+// Tickets: first the group's IBM tasks, then its tiles, so the
 // forward-progress argument of lbm_substep_kernel carries over (a tile waits
 // only for IBM tasks of its own system, all of which have lower tickets).
-__global__ void __launch_bounds__(kTile, 768 / kTile) lbm_substep_batch_kernel(BatchLaunch L) {
+template <int ST, int PARITY, int PERX, bool DET>
+__global__ void __launch_bounds__(kTile, (batch_ctas_per_sm<ST, PARITY>())) lbm_substep_batch_kernel(BatchLaunch L) {
     __shared__ BatchSlot s_slot[2];
     // programmatic dependent launch as in lbm_substep_kernel (from the second
     // substep of an iteration on)
@@ -1174,22 +1175,33 @@ __global__ void __launch_bounds__(kTile, 768 / kTile) lbm_substep_batch_kernel(B
         } else if (sl.is_ibm) {
             ibm_task(sl.a, sl.local);
         } else {
-            const int st = sl.a.F.storage;
-            if (sl.a.F.det_spread) {
-                if (st == kStoreF32) batch_tile<kStoreF32, true>(sl);
-                else if (st == kStoreF16) batch_tile<kStoreF16, true>(sl);
-                else batch_tile<kStoreBF16, true>(sl);
-            } else {
-                if (st == kStoreF32) batch_tile<kStoreF32, false>(sl);
-                else if (st == kStoreF16) batch_tile<kStoreF16, false>(sl);
-                else batch_tile<kStoreBF16, false>(sl);
-            }
+            lbm_tile<ST, PARITY, PERX, true, DET>(sl.a, sl.local, sl.ts);
         }
         if (warp0) {
             tn = __shfl_sync(0xffffffffu, tn, 0);
             prepare_batch_slot(L, tn, s_slot[j ^ 1]);
         }
         __syncthreads();
+    }
+}
+
+using BatchKernel = void (*)(BatchLaunch);
+
+// the group instantiation; even substeps move no population across a cell
+// boundary, so they have no x-periodic form
+template <int ST>
+BatchKernel batch_kernel_of(int parity, int perx, int det) {
+    if (!parity) return det ? lbm_substep_batch_kernel<ST, 0, 0, true> : lbm_substep_batch_kernel<ST, 0, 0, false>;
+    if (perx) return det ? lbm_substep_batch_kernel<ST, 1, 1, true> : lbm_substep_batch_kernel<ST, 1, 1, false>;
+    return det ? lbm_substep_batch_kernel<ST, 1, 0, true> : lbm_substep_batch_kernel<ST, 1, 0, false>;
+}
+
+BatchKernel batch_kernel(int storage, int parity, int perx, int det) {
+    switch (storage) {
+        case kStoreF32: return batch_kernel_of<kStoreF32>(parity, perx, det);
+        case kStoreF16: return batch_kernel_of<kStoreF16>(parity, perx, det);
+        case kStoreBF16: return batch_kernel_of<kStoreBF16>(parity, perx, det);
+        default: return nullptr;
     }
 }
 
@@ -1490,8 +1502,10 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_substep_batch(const BatchLaunch& L, int grid, cudaStream_t s) {
+cudaError_t launch_substep_batch(const BatchLaunch& L, const BatchGroupKey& g, int parity, int grid, cudaStream_t s) {
     static const bool no_pdl = getenv("GLSM_NO_PDL") != nullptr;
+    const BatchKernel k = batch_kernel(g.storage, parity, g.perx, g.det);
+    if (!k) return cudaErrorInvalidValue;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = (no_pdl || L.k == 0) ? 0 : 1;
@@ -1501,7 +1515,7 @@ cudaError_t launch_substep_batch(const BatchLaunch& L, int grid, cudaStream_t s)
     cfg.stream = s;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, lbm_substep_batch_kernel, L);
+    return cudaLaunchKernelEx(&cfg, k, L);
 }
 
 cudaError_t launch_conv_diff_batch(const BatchSys* sys, const int* block_offsets, int n, int blocks, cudaStream_t s) {
@@ -1516,11 +1530,12 @@ cudaError_t launch_batch_advance(const BatchSys* sys, int n, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-int batch_resident_ctas() {
+int batch_resident_ctas(const BatchGroupKey& g, int parity) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_batch_kernel, kTile, 0);
+    const BatchKernel k = batch_kernel(g.storage, parity, g.perx, g.det);
+    if (k) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTile, 0);
     return max(1, sms * max(1, per_sm));
 }
 

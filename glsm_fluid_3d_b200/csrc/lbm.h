@@ -40,22 +40,31 @@ struct BatchSys {
     SysDyn* dyn;
 };
 
-// one batched substep launch
+// one batched substep launch: the n systems of one group
 struct BatchLaunch {
-    const BatchSys* sys;
-    const int* ibm_offsets;   // [n + 1] prefix sums of IBM tasks per system
-    const int* tile_offsets;  // [n + 1] prefix sums of lattice tiles per system
-    unsigned* tickets;        // [nsub] batch-wide ticket counters
+    const BatchSys* sys;      // every system of the batch
+    const int* members;       // [n] index into sys of each system of the group
+    const int* ibm_offsets;   // [n + 1] prefix sums of IBM tasks per group system
+    const int* tile_offsets;  // [n + 1] prefix sums of lattice tiles per group system
+    unsigned* tickets;        // [nsub] the group's ticket counters
     int n;
     int k;
     int last;
 };
 
+// what a group's systems share: one kernel instantiation serves them all
+// (their substep parity is shared too and chosen per launch)
+struct BatchGroupKey {
+    int storage;
+    int perx;  // periodic in x
+    int det;   // deterministic spreads
+};
+
 int lbm_grid(const StepArgs& a, int parity);
-cudaError_t launch_substep_batch(const BatchLaunch& L, int grid, cudaStream_t s);
+cudaError_t launch_substep_batch(const BatchLaunch& L, const BatchGroupKey& g, int parity, int grid, cudaStream_t s);
 cudaError_t launch_conv_diff_batch(const BatchSys* sys, const int* block_offsets, int n, int blocks, cudaStream_t s);
 cudaError_t launch_batch_advance(const BatchSys* sys, int n, cudaStream_t s);
-int batch_resident_ctas();
+int batch_resident_ctas(const BatchGroupKey& g, int parity);
 int lbm_resident_ctas(int storage, int parity);
 void staged_setup(int* ctas32, int* ctas16);
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s);

@@ -2,7 +2,8 @@
 
 A system's result must be the same alone and in the mix: systems of different
 lattice sizes, gel counts and storages advanced together by one batch (one
-persistent launch per substep for all of them), including a system that joins
+persistent launch per substep for each group of systems that share storage
+and substep parity), including a system that joins
 while the others are running, agree with the same systems advanced alone.  The
 spreads use float atomics, so agreement is to round-off (relative L2 <= 1e-5)
 for FP32 storage and to FP16 precision for FP16 storage.

@@ -96,3 +96,53 @@ def test_deterministic_same_alone_and_in_batch(gpu):
         b.remove(s.fluid)
         s.close()
     b.close()
+
+
+def test_deterministic_same_alone_and_in_a_mixed_batch(gpu):
+    """The batch launches its systems in groups (storage, x periodicity,
+    substep parity); one batch holding every kind, with systems that join with
+    an odd substep count after running alone first, still reproduces each
+    system alone bit for bit."""
+    from glsm_fluid_3d_b200 import Batch, System
+
+    # (dims, gel position, storage, periodic, iterations alone before joining)
+    specs = [((20, 18, 22), (4.75, 4.25, 5.25), "f32", (0, 0, 0), 0),
+             ((24, 20, 16), (5.75, 4.75, 3.75), "f16", (0, 0, 0), 1),
+             ((18, 22, 20), (4.25, 5.75, 4.75), "bf16", (1, 0, 0), 0),
+             ((22, 16, 18), (5.25, 3.75, 4.25), "f32", (1, 0, 1), 1),
+             ((16, 24, 20), (3.75, 5.25, 4.75), "f16", (1, 0, 0), 2)]
+
+    def make(dims, pos, storage, periodic, seed):
+        s = System(*dims, nsub=3, storage=storage, deterministic=True)
+        s.add_gel((3, 3, 3), pos, 1, 1)
+        s.gel_noise(0, seed, 1e-3)
+        s.set_params(beta=1.0, ramp_steps=0.0, periodic=periodic)
+        s.finalize()
+        return s
+
+    total = 7
+    alone = []
+    for k, (dims, pos, storage, per, pre) in enumerate(specs):
+        s = make(dims, pos, storage, per, 20 + k)
+        s.run(0, total)
+        alone.append((s.fluid.read("u"), s.fluid.read("pop"), s.gels[0].read("rn")))
+        s.close()
+    systems = []
+    b = Batch()
+    for k, (dims, pos, storage, per, pre) in enumerate(specs):
+        s = make(dims, pos, storage, per, 20 + k)
+        if pre:
+            s.run(0, pre)
+        s.fluid.sync()
+        b.add(s.fluid, pre, total - pre)
+        systems.append(s)
+    b.run(total)
+    b.sync()
+    for k, (s, want) in enumerate(zip(systems, alone)):
+        got = (s.fluid.read("u"), s.fluid.read("pop"), s.gels[0].read("rn"))
+        for name, g, w in zip(("u", "pop", "rn"), got, want):
+            assert np.array_equal(g, w), (k, specs[k][2], name)
+    for s in systems:
+        b.remove(s.fluid)
+        s.close()
+    b.close()
