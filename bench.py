@@ -68,6 +68,8 @@ W = WORKLOADS["D"]
 DIMS, NSUB = W["dims"], W["nsub"]
 BYTES_PER_CELL = {"f32": 152, "f16": 76, "bf16": 76}  # one read + one write of 19 populations
 FLUSH_BYTES = 256 << 20  # > the 126 MB L2
+L2_PROBE_BYTES = 24 << 20  # two buffers: a 48 MiB footprint, inside the 126 MB L2
+L2_PROBE_REPS = 400
 
 
 def parse():
@@ -318,8 +320,16 @@ def run_ours(args, world, rank, local):
     achieved = bpc * N / (avg_ms / 1e3) / 1e9
     peak, peak_kind = peaks()
     traffic = ncu_traffic(args.storage)
+    # one population copy of 101^3 (78 MB FP32, 39 MB FP16) fits in L2: the
+    # achieved bandwidth is also set against a measured L2 copy bandwidth
+    from glsm_fluid_3d_b200 import copy_bandwidth
+
+    l2 = copy_bandwidth(L2_PROBE_BYTES, L2_PROBE_REPS)
     roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
             "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
+            "l2_peak": round(l2, 1), "frac_l2": round(achieved / l2, 4),
+            "l2_peak_how": f"glsm_copy_bandwidth: 2 x {L2_PROBE_BYTES >> 20} MiB copied back and forth "
+                           f"{L2_PROBE_REPS} times in one launch, L1 bypassed (measured in this run)",
             "kernel": "lbm_substep_kernel", "bytes_per_launch": bpc * N, "avg_launch_ms": round(avg_ms, 5),
             "avg_launch_ms_event_pairs": round(statistics.mean(prof), 5),
             "timing": "3 velocity steps, each a captured graph of its substep launches between one event pair, "

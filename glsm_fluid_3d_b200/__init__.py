@@ -27,7 +27,7 @@ import numpy as np
 
 from ._lib import FluidDesc, GlsmError, check, lib
 
-__all__ = ["Gel", "Coupler", "Fluid", "System", "Batch", "GlsmError", "STORAGE", "lib"]
+__all__ = ["Gel", "Coupler", "Fluid", "System", "Batch", "GlsmError", "STORAGE", "lib", "copy_bandwidth"]
 
 STORAGE = {"f32": 0, "fp32": 0, "f16": 1, "fp16": 1, "bf16": 2}
 
@@ -38,6 +38,19 @@ GEL_FIELDS = {
 }
 FLUID_FIELDS = {"pop": 0, "rho": 1, "u": 2, "c1": 3}
 MARKER_FIELDS = {"lag": 0, "Ul": 1, "Vl": 2, "Fdrag": 3, "Frep": 4, "Cl": 5, "Dl": 6, "Sl": 7}
+
+
+def copy_bandwidth(nbytes: int, reps: int) -> float:
+    """Measured copy bandwidth in GB/s (read + write bytes): a buffer of nbytes
+    copied back and forth reps times in one launch through L2 only.  With
+    2 x nbytes well below the 126 MB L2 this is the L2 copy bandwidth, well
+    above it the HBM copy bandwidth (glsm_copy_bandwidth)."""
+    L = lib()
+    out = ctypes.c_double(0.0)
+    rc = L.glsm_copy_bandwidth(int(nbytes), int(reps), ctypes.byref(out))
+    if rc != 0:
+        raise GlsmError(f"copy_bandwidth: {L.glsm_copy_bandwidth_error().decode()}")
+    return out.value
 
 
 def _dptr(a):

@@ -98,6 +98,9 @@ def lib():
     L.glsm_batch_remaining.restype = ctypes.c_longlong
     L.glsm_coupler_stream.argtypes = [vp]
     L.glsm_coupler_stream.restype = vp
+    L.glsm_copy_bandwidth.argtypes = [ctypes.c_size_t, i, P(d)]
+    L.glsm_copy_bandwidth.restype = i
+    L.glsm_copy_bandwidth_error.restype = ctypes.c_char_p
     _lib = L
     return L
 

@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libglsm_b200.so")
-SOURCES = ["lbm.cu", "gel.cu", "capi.cu", "noalloc.cu", "dropin.cpp"]
+SOURCES = ["lbm.cu", "gel.cu", "capi.cu", "noalloc.cu", "bandwidth.cu", "dropin.cpp"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo",
               "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr"]
 

@@ -252,6 +252,17 @@ int glsm_fluid_profile_substeps(glsm_fluid f, int iter, float* total_ms);
 /* gel_to_lbm_vel and lbm_to_gel_vel (src/fluid.cu:221-222) */
 int glsm_fluid_units(glsm_fluid f, float out[2]);
 
+/* Copy-bandwidth probe (extension: a measurement aid with no counterpart in
+ * the reference).  Copies a `bytes`-sized buffer back and forth `reps` times in
+ * one launch through L2 only (L1 bypassed) and stores read + write bytes per
+ * second in *gbs (GB/s).  With 2 x bytes well below the L2 size this is the
+ * L2 copy bandwidth the substep kernel is compared with when the population
+ * array fits in L2; with 2 x bytes well above it, the HBM copy bandwidth.
+ * Allocates and frees its two buffers; bytes a multiple of 16 in [16, 8 GiB],
+ * reps in [1, 100000].  glsm_copy_bandwidth_error() explains a failure. */
+int glsm_copy_bandwidth(size_t bytes, int reps, double* gbs);
+const char* glsm_copy_bandwidth_error(void);
+
 /* ---- Batch: several systems advanced together -----------------------------
  * No single counterpart in the reference (which runs one system per process);
  * this is the serving form of Fluid::stepVelocity & co.  Systems (fluid handles

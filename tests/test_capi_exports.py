@@ -59,3 +59,16 @@ def test_fluid_desc_defaults_match_reference_constants():
     assert abs(d.tau - 0.8) < 1e-7 and abs(d.h - 0.5) < 1e-7
     assert d.beta == 1.0 and d.ramp_steps == 20000.0
     assert d.storage == 0
+
+
+def test_copy_bandwidth_rejects_bad_sizes():
+    """Arguments are checked before any CUDA call, so this runs without a GPU."""
+    import ctypes
+
+    from glsm_fluid_3d_b200 import lib
+
+    L = lib()
+    out = ctypes.c_double(0.0)
+    for nbytes, reps in ((0, 1), (17, 1), (1 << 20, 0), (1 << 20, 100001), ((8 << 30) + 16, 1)):
+        assert L.glsm_copy_bandwidth(nbytes, reps, ctypes.byref(out)) == -1, (nbytes, reps)
+    assert b"multiple of 16" in L.glsm_copy_bandwidth_error()
