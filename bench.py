@@ -66,7 +66,7 @@ WORKLOADS = {
 }
 W = WORKLOADS["D"]
 DIMS, NSUB = W["dims"], W["nsub"]
-BYTES_PER_CELL = {"f32": 152, "f16": 76, "bf16": 76}  # one read + one write of 19 populations
+BYTES_PER_CELL = {"f32": 152, "f16": 76, "bf16": 76, "f16c": 76, "f16c2": 76}  # one read + one write of 19 populations
 FLUSH_BYTES = 256 << 20  # > the 126 MB L2
 L2_PROBE_BYTES = 24 << 20  # two buffers: a 48 MiB footprint, inside the 126 MB L2
 L2_PROBE_REPS = 400
@@ -78,7 +78,9 @@ def parse():
     p.add_argument("--steps", type=int, default=1000)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f16c", "f16c2"],
+                   help="f16c / f16c2: FP16 storage with the mass- and momentum-conserving rounding on every / "
+                        "every second substep")
     p.add_argument("--workload", default="D", choices=sorted(WORKLOADS),
                    help="D: 101^3 two gels (default); S: 48^3 one gel; P: 256^3 eight gels; L: 384x384x192 rods")
     p.add_argument("--no-cpu-baseline", action="store_true")

@@ -29,7 +29,12 @@ from ._lib import FluidDesc, GlsmError, check, lib
 
 __all__ = ["Gel", "Coupler", "Fluid", "System", "Batch", "GlsmError", "STORAGE", "lib", "copy_bandwidth"]
 
-STORAGE = {"f32": 0, "fp32": 0, "f16": 1, "fp16": 1, "bf16": 2}
+STORAGE = {"f32": 0, "fp32": 0, "f16": 1, "fp16": 1, "bf16": 2, "f16c": 1, "f16c2": 1}
+# FP16 rounding modes (glsm_fluid_set_f16_rounding); storage "f16c" is FP16
+# storage with the conserving rounding on every substep, "f16c2" on every
+# second (odd) substep
+F16_ROUNDING = {"nearest": 0, "conserving": 1, "conserving_odd": 2}
+_STORAGE_ROUNDING = {"f16c": "conserving", "f16c2": "conserving_odd"}
 
 GEL_FIELDS = {
     "rn": 0, "Veln": 1, "Vels": 2, "Fn": 3, "um": 4, "vm": 5, "wm": 6, "un_norm": 7, "vn_norm": 8,
@@ -226,12 +231,14 @@ class Fluid:
 
     `dims` are lattice cells per axis (the reference derives 2*s+1 from a
     physical size s; any size is accepted here).  Keyword overrides: nsub,
-    storage ("f32" | "f16" | "bf16"), tau, beta, ramp_steps, force, periodic,
-    fp16_scale, h; deterministic=True spreads by fixed-order gathers (a run
-    repeats bit for bit) instead of float atomics.
+    storage ("f32" | "f16" | "bf16" | "f16c" | "f16c2": FP16 with the
+    conserving rounding on every / every second substep), tau, beta, ramp_steps, force, periodic, fp16_scale, h;
+    deterministic=True spreads by fixed-order gathers (a run repeats bit for
+    bit) instead of float atomics.
     """
 
     def __init__(self, dims, coupler, deterministic=False, **kw):
+        rounding = _STORAGE_ROUNDING.get(kw.get("storage"))
         self.L = lib()
         d = FluidDesc()
         check(self.L.glsm_fluid_desc_default(ctypes.byref(d), int(dims[0]), int(dims[1]), int(dims[2])), "desc")
@@ -257,6 +264,14 @@ class Fluid:
         self.nx, self.ny, self.nz, self.N, self.Nsub, self.storage, self.device_bytes, _ = (int(v) for v in info)
         if deterministic:
             self.set_deterministic(True)
+        if rounding:
+            self.set_f16_rounding(rounding)
+
+    def set_f16_rounding(self, mode="conserving"):
+        """Rounding of FP16 storage: "nearest", "conserving" (each cell's
+        mass and momentum rounding errors nearly cancel) or "conserving_odd"
+        (conserving on odd substeps only); glsm_fluid_set_f16_rounding."""
+        check(self.L.glsm_fluid_set_f16_rounding(self.h, F16_ROUNDING[mode]), "set_f16_rounding")
 
     def set_deterministic(self, on=True):
         """Spreads as fixed-order gathers (glsm_fluid_set_deterministic)."""

@@ -924,8 +924,8 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     }
     int nsub_phys;
     fluid_units(d->tau, d->h, c->g2l, c->l2g, nsub_phys);
-    f->lbm_ctas = lbm_resident_ctas(d->storage, 1);
-    f->lbm_ctas_even = lbm_resident_ctas(d->storage, 0);
+    f->lbm_ctas = lbm_resident_ctas(d->storage, 1, 0);
+    f->lbm_ctas_even = lbm_resident_ctas(d->storage, 0, 0);
     {
         static int ctas32 = -1, ctas16 = -1;  // per process (one device type)
         if (ctas32 < 0) staged_setup(&ctas32, &ctas16);
@@ -968,6 +968,41 @@ int glsm_fluid_set_deterministic(glsm_fluid f, int on) {
                 cudaGraphExecDestroy(g);
                 g = nullptr;
             }
+    return GLSM_OK;
+}
+
+int glsm_fluid_set_f16_rounding(glsm_fluid f, int mode) {
+    if (!f) return fail(GLSM_ERR_ARG, "null fluid");
+    if (mode < 0 || mode > 2)
+        return fail(GLSM_ERR_ARG, "rounding mode %d: 0 nearest, 1 conserving, 2 conserving on odd substeps", mode);
+    if (mode && f->F.storage != GLSM_STORE_F16) return fail(GLSM_ERR_ARG, "conserving rounding needs FP16 storage");
+    if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
+    CK(cudaStreamSynchronize(f->c->stream));
+    f->F.f16_round = mode;
+    f->lbm_ctas = lbm_resident_ctas(f->F.storage, 1, mode);
+    f->lbm_ctas_even = lbm_resident_ctas(f->F.storage, 0, mode);
+    // the captured iteration graphs hold the old launch arguments
+    for (auto& row : f->graph)
+        for (auto& g : row)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    return GLSM_OK;
+}
+
+int glsm_f16_conserve_round(const float* in, float* out, size_t n_cells) {
+    if (!in || !out) return fail(GLSM_ERR_ARG, "null argument");
+    if (n_cells == 0) return GLSM_OK;
+    if (n_cells > ((size_t)1 << 26)) return fail(GLSM_ERR_ARG, "at most 2^26 cells per call");
+    const size_t bytes = n_cells * 19 * sizeof(float);
+    float* d = nullptr;
+    CK(cudaMalloc(&d, 2 * bytes));
+    cudaError_t e = cudaMemcpy(d, in, bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_conserve_round(d, d + n_cells * 19, (long long)n_cells, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + n_cells * 19, bytes, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(GLSM_ERR_CUDA, "conserve_round: %s", cudaGetErrorString(e));
     return GLSM_OK;
 }
 
@@ -1367,10 +1402,11 @@ static int batch_rebuild(glsm_batch_s* b) {
     std::vector<Group> groups;
     for (int i = 0; i < n; i++) {
         const glsm_fluid_s* f = b->sys[i];
-        const BatchGroupKey key{f->F.storage, f->F.per[0], f->F.det_spread};
+        const BatchGroupKey key{f->F.storage, f->F.per[0], f->F.det_spread, f->F.f16_round};
         const int p0 = (int)(f->substeps & 1);
         auto it = std::find_if(groups.begin(), groups.end(), [&](const Group& g) {
-            return g.key.storage == key.storage && g.key.perx == key.perx && g.key.det == key.det && g.p0 == p0;
+            return g.key.storage == key.storage && g.key.perx == key.perx && g.key.det == key.det &&
+                   g.key.f16_round == key.f16_round && g.p0 == p0;
         });
         if (it == groups.end()) {
             groups.push_back(Group{key, p0, {}});

@@ -122,6 +122,7 @@ struct FluidDev {
     float beta, ramp_steps;
     int nsub;
     int det_spread;  // spreads as fixed-order gathers instead of float atomics
+    int f16_round;   // FP16 storage: 0 round to nearest, 1 conserving rounding, 2 conserving on odd substeps
     long long substeps_done;  // host-side bookkeeping of the AA parity
 };
 

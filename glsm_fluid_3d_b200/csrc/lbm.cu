@@ -27,12 +27,24 @@ namespace glsm {
 // ---------------------------------------------------------------------------
 // population storage: FP32 deviations, or FP16 / BF16 deviations (scaled)
 // ---------------------------------------------------------------------------
+// FP16 storage with the conserving rounding of conserve_round: a template
+// value of the substep kernels only (the fluid's storage stays kStoreF16 and
+// FluidDev::f16_round selects these instantiations)
+constexpr int kStoreF16C = 3;
+
+// whether a substep of this parity rounds conservingly under FP16 rounding
+// mode f16_round (0 nearest, 1 every substep, 2 odd substeps only)
+__host__ __device__ constexpr bool f16_conserving(int f16_round, int parity) {
+    return f16_round == 1 || (f16_round == 2 && parity != 0);
+}
+
 template <int ST>
 struct PopIO;
 template <>
 struct PopIO<kStoreF32> {
     using T = float;
     static constexpr bool kScaled = false;
+    static constexpr bool kConserve = false;
     static __device__ __forceinline__ float ld(const T* p, float) { return *p; }
     static __device__ __forceinline__ void st(T* p, float v, float) { *p = v; }
     static __device__ __forceinline__ float raw(const T* p) { return *p; }
@@ -42,6 +54,7 @@ template <>
 struct PopIO<kStoreF16> {
     using T = __half;
     static constexpr bool kScaled = true;  // stored value = deviation * scale
+    static constexpr bool kConserve = false;
     static __device__ __forceinline__ float ld(const T* p, float inv_scale) { return __half2float(*p) * inv_scale; }
     static __device__ __forceinline__ void st(T* p, float v, float scale) { *p = __float2half_rn(v * scale); }
     static __device__ __forceinline__ float raw(const T* p) { return __half2float(*p); }
@@ -55,8 +68,14 @@ struct PopIO<kStoreBF16> {
     }
     static __device__ __forceinline__ void st(T* p, float v, float scale) { *p = __float2bfloat16_rn(v * scale); }
     static constexpr bool kScaled = false;  // stored unscaled
+    static constexpr bool kConserve = false;
     static __device__ __forceinline__ float raw(const T* p) { return __bfloat162float(*p); }
     static __device__ __forceinline__ void st_raw(T* p, float v) { *p = __float2bfloat16_rn(v); }
+};
+
+template <>
+struct PopIO<kStoreF16C> : PopIO<kStoreF16> {
+    static constexpr bool kConserve = true;
 };
 
 // Two adjacent cells' populations of one direction as one vector (the even
@@ -102,6 +121,8 @@ struct PairIO<kStoreBF16> {
     static __device__ __forceinline__ V set_lo_raw(V v, __nv_bfloat16 a) { return __halves2bfloat162(a, __high2bfloat16(v)); }
     static __device__ __forceinline__ V set_hi_raw(V v, __nv_bfloat16 b) { return __halves2bfloat162(__low2bfloat16(v), b); }
 };
+template <>
+struct PairIO<kStoreF16C> : PairIO<kStoreF16> {};
 
 __device__ __forceinline__ int current_iter(int iter_arg, const Ctl* ctl) {
     return iter_arg >= 0 ? iter_arg : ctl->iter;
@@ -430,6 +451,60 @@ __device__ __forceinline__ void collide(float (&d)[19], float Fhx, float Fhy, fl
     collide_pair<16>(d, t);
 }
 
+// Conserving FP16 rounding of one cell's 19 scaled post-collision values.
+// With round-to-nearest every cell emits a random mass and momentum error each
+// substep; summed over the lattice these errors excite long-wavelength
+// acoustic and shear modes that viscosity damps slowly, and over thousands of
+// steps that accumulated noise, not the rounding of the current step,
+// dominates the velocity error.  Here every value is first rounded to
+// nearest; then, direction by direction (1..18), a value moves to its other
+// FP16 neighbour (one FP16 spacing towards the exact value) when that lowers
+// M^2 + |P|^2, M and P being the cell's summed mass and momentum rounding
+// errors so far.  What a cell emits then carries almost no mass or momentum
+// error, so the injected noise is a divergence of per-cell errors and sits at
+// short wavelengths, which viscosity removes within a few steps.  d[q]
+// receives the float value of the chosen FP16 number (exactly representable,
+// so the store's round-to-nearest conversion reproduces it).  The arithmetic
+// uses explicitly rounded intrinsics, so the result does not depend on FMA
+// contraction and a float32 restatement reproduces it bit for bit.
+__device__ __forceinline__ void conserve_round(float (&d)[19]) {
+    float e[19];
+    float M = 0.f, Px = 0.f, Py = 0.f, Pz = 0.f;
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        const float h = __half2float(__float2half_rn(d[q]));
+        e[q] = __fsub_rn(d[q], h);
+        d[q] = h;
+        M = __fadd_rn(M, e[q]);
+        if (qcx(q)) Px = qcx(q) > 0 ? __fadd_rn(Px, e[q]) : __fsub_rn(Px, e[q]);
+        if (qcy(q)) Py = qcy(q) > 0 ? __fadd_rn(Py, e[q]) : __fsub_rn(Py, e[q]);
+        if (qcz(q)) Pz = qcz(q) > 0 ? __fadd_rn(Pz, e[q]) : __fsub_rn(Pz, e[q]);
+    }
+#pragma unroll
+    for (int q = 1; q < 19; q++) {
+        const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
+        // FP16 spacing at d[q]: 2^(exponent - 10), 2^-24 below the normal
+        // range.  At a power of two reached from below the step down is twice
+        // the spacing there, which still lands on an FP16 number.
+        const float ulp = fmaxf(__int_as_float((__float_as_int(d[q]) & 0x7f800000) - (10 << 23)), 0x1p-24f);
+        const float de = copysignf(ulp, -e[q]);  // change of e[q] if d[q] moves
+        float t = M;
+        if (cx) t = cx > 0 ? __fadd_rn(t, Px) : __fsub_rn(t, Px);
+        if (cy) t = cy > 0 ? __fadd_rn(t, Py) : __fsub_rn(t, Py);
+        if (cz) t = cz > 0 ? __fadd_rn(t, Pz) : __fsub_rn(t, Pz);
+        // change of M^2 + |P|^2: de (2 t + (1 + |c|^2) de)
+        const float k = (float)(1 + cx * cx + cy * cy + cz * cz);
+        const float s = __fadd_rn(__fmul_rn(2.0f, t), __fmul_rn(k, de));
+        if (__fmul_rn(de, s) < 0.0f) {
+            d[q] = __fsub_rn(d[q], de);
+            M = __fadd_rn(M, de);
+            if (cx) Px = cx > 0 ? __fadd_rn(Px, de) : __fsub_rn(Px, de);
+            if (cy) Py = cy > 0 ? __fadd_rn(Py, de) : __fsub_rn(Py, de);
+            if (cz) Pz = cz > 0 ? __fadd_rn(Pz, de) : __fsub_rn(Pz, de);
+        }
+    }
+}
+
 // body force (uniform F_const plus, inside the marker boxes, the IBM force,
 // which the cell consumes) and collision; returns (ux, uy, uz, rho)
 template <int ST>
@@ -467,6 +542,7 @@ __device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, u
     T* P = reinterpret_cast<T*>(F.pop);
     const long long LS = S, Lnx = nx, Lnxy = nxy;
     const float4 u = force_collide<ST>(a, i, inb, d);
+    if constexpr (IO::kConserve) conserve_round(d);
 
     T* Pi = P + i;
     if (PARITY == 0) {
@@ -673,6 +749,7 @@ __device__ __forceinline__ void lbm_pair_even(const StepArgs& a, unsigned i0, bo
 #pragma unroll
         for (int q = 0; q < 19; q++) d[q] = PIO::lo(r[q]);
         store_u(a, i0, inb0, force_collide<ST>(a, i0, inb0, d));
+        if constexpr (PopIO<ST>::kConserve) conserve_round(d);
 #pragma unroll
         for (int q = 0; q < 19; q++) r[q] = PIO::set_lo(r[q], d[q]);
     }
@@ -681,6 +758,7 @@ __device__ __forceinline__ void lbm_pair_even(const StepArgs& a, unsigned i0, bo
 #pragma unroll
         for (int q = 0; q < 19; q++) d[q] = PIO::hi(r[q]);
         store_u(a, i0 + 1, inb1, force_collide<ST>(a, i0 + 1, inb1, d));
+        if constexpr (PopIO<ST>::kConserve) conserve_round(d);
 #pragma unroll
         for (int q = 0; q < 19; q++) r[q] = PIO::set_hi(r[q], d[q]);
     }
@@ -722,7 +800,7 @@ __device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const
     const unsigned c1 = min(c0 + kTileCells - 1, (unsigned)F.N - 1);
     const int nb = sl.nb;
     if (nb > 0) wait_ibm(a);
-    if constexpr (PAIR && PARITY == 0 && ST == kStoreF16 && kCellsPerThread == 2) {
+    if constexpr (PAIR && PARITY == 0 && (ST == kStoreF16 || ST == kStoreF16C) && kCellsPerThread == 2) {
         const unsigned i0 = c0 + 2 * threadIdx.x;
         const bool inb0 = nb > 0 && i0 <= c1 && in_boxes<DET>(a, sl, nb, i0);
         const bool inb1 = nb > 0 && i0 + 1 <= c1 && in_boxes<DET>(a, sl, nb, i0 + 1);
@@ -751,7 +829,7 @@ template <int ST, int PARITY>
 constexpr int lbm_ctas_per_sm() {
     // 64 registers (4 CTAs of 256 threads per SM); 80 (3 CTAs) for the paired
     // even substeps of FP16 storage, whose threads hold two cells
-    return (PARITY == 0 && ST == kStoreF16) ? 768 / kTile : 1024 / kTile;
+    return (PARITY == 0 && (ST == kStoreF16 || ST == kStoreF16C)) ? 768 / kTile : 1024 / kTile;
 }
 
 template <int ST, int PARITY, int PERX, bool DET>
@@ -1196,10 +1274,12 @@ BatchKernel batch_kernel_of(int parity, int perx, int det) {
     return det ? lbm_substep_batch_kernel<ST, 1, 0, true> : lbm_substep_batch_kernel<ST, 1, 0, false>;
 }
 
-BatchKernel batch_kernel(int storage, int parity, int perx, int det) {
+BatchKernel batch_kernel(int storage, int parity, int perx, int det, int f16_round) {
     switch (storage) {
         case kStoreF32: return batch_kernel_of<kStoreF32>(parity, perx, det);
-        case kStoreF16: return batch_kernel_of<kStoreF16>(parity, perx, det);
+        case kStoreF16:
+            return f16_conserving(f16_round, parity) ? batch_kernel_of<kStoreF16C>(parity, perx, det)
+                                                     : batch_kernel_of<kStoreF16>(parity, perx, det);
         case kStoreBF16: return batch_kernel_of<kStoreBF16>(parity, perx, det);
         default: return nullptr;
     }
@@ -1430,11 +1510,15 @@ int lbm_grid(const StepArgs& a, int parity) {
     return ctas > 0 ? min(total, ctas) : total;
 }
 
-int lbm_resident_ctas(int storage, int parity) {
+int lbm_resident_ctas(int storage, int parity, int f16_round) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (storage == kStoreF16 && parity == 0)
+    if (storage == kStoreF16 && f16_conserving(f16_round, parity) && parity == 0)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF16C, 0, 0, false>, kTile, 0);
+    else if (storage == kStoreF16 && f16_conserving(f16_round, parity))
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF16C, 1, 0, false>, kTile, 0);
+    else if (storage == kStoreF16 && parity == 0)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF16, 0, 0, false>, kTile, 0);
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF32, 1, 0, false>, kTile, 0);
@@ -1442,7 +1526,7 @@ int lbm_resident_ctas(int storage, int parity) {
 }
 
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
-    if (a.staged_ctas > 0) {
+    if (a.staged_ctas > 0 && a.F.f16_round == 0) {
         const int total = a.n_ibm + a.n_tiles;
         const dim3 g(min(total, a.staged_ctas)), b(kTile);
 #define GLSM_STAGED(ST)                                                                          \
@@ -1493,7 +1577,13 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
     }
     switch (a.F.storage) {
         case kStoreF32: GLSM_SUB(kStoreF32); break;
-        case kStoreF16: GLSM_SUB(kStoreF16); break;
+        case kStoreF16:
+            if (f16_conserving(a.F.f16_round, parity)) {
+                GLSM_SUB(kStoreF16C);
+            } else {
+                GLSM_SUB(kStoreF16);
+            }
+            break;
         case kStoreBF16: GLSM_SUB(kStoreBF16); break;
         default: return cudaErrorInvalidValue;
     }
@@ -1504,7 +1594,7 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
 
 cudaError_t launch_substep_batch(const BatchLaunch& L, const BatchGroupKey& g, int parity, int grid, cudaStream_t s) {
     static const bool no_pdl = getenv("GLSM_NO_PDL") != nullptr;
-    const BatchKernel k = batch_kernel(g.storage, parity, g.perx, g.det);
+    const BatchKernel k = batch_kernel(g.storage, parity, g.perx, g.det, g.f16_round);
     if (!k) return cudaErrorInvalidValue;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -1534,7 +1624,7 @@ int batch_resident_ctas(const BatchGroupKey& g, int parity) {
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const BatchKernel k = batch_kernel(g.storage, parity, g.perx, g.det);
+    const BatchKernel k = batch_kernel(g.storage, parity, g.perx, g.det, g.f16_round);
     if (k) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTile, 0);
     return max(1, sms * max(1, per_sm));
 }
@@ -1579,6 +1669,25 @@ cudaError_t launch_write_pop(const FluidDev& F, const float* in, cudaStream_t s)
         case kStoreBF16: write_pop_kernel<kStoreBF16><<<grid, block, 0, s>>>(F, in); break;
         default: return cudaErrorInvalidValue;
     }
+    return cudaGetLastError();
+}
+
+// conserve_round over n cells of 19 values each ([cell][direction]), for the
+// bit-for-bit check against its float32 restatement
+__global__ void conserve_round_kernel(const float* in, float* out, long long n) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n) return;
+    float d[19];
+#pragma unroll
+    for (int q = 0; q < 19; q++) d[q] = in[c * 19 + q];
+    conserve_round(d);
+#pragma unroll
+    for (int q = 0; q < 19; q++) out[c * 19 + q] = d[q];
+}
+
+cudaError_t launch_conserve_round(const float* in, float* out, long long n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    conserve_round_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(in, out, n);
     return cudaGetLastError();
 }
 

@@ -58,6 +58,7 @@ struct BatchGroupKey {
     int storage;
     int perx;  // periodic in x
     int det;   // deterministic spreads
+    int f16_round;  // FP16 rounding mode (0 nearest, 1 conserving, 2 conserving on odd substeps)
 };
 
 int lbm_grid(const StepArgs& a, int parity);
@@ -65,7 +66,7 @@ cudaError_t launch_substep_batch(const BatchLaunch& L, const BatchGroupKey& g, i
 cudaError_t launch_conv_diff_batch(const BatchSys* sys, const int* block_offsets, int n, int blocks, cudaStream_t s);
 cudaError_t launch_batch_advance(const BatchSys* sys, int n, cudaStream_t s);
 int batch_resident_ctas(const BatchGroupKey& g, int parity);
-int lbm_resident_ctas(int storage, int parity);
+int lbm_resident_ctas(int storage, int parity, int f16_round);
 void staged_setup(int* ctas32, int* ctas16);
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s);
 cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s);
@@ -74,6 +75,8 @@ cudaError_t launch_write_pop(const FluidDev& F, const float* in, cudaStream_t s)
 // global mass and momentum in FP64 (deterministic two-pass reduction); `partial`
 // holds kConsBlocks x 4 doubles, `out` receives sum(rho), sum(c f) x, y, z
 constexpr int kConsBlocks = 296;
+// the conserving FP16 rounding of n cells ([cell][19] device arrays)
+cudaError_t launch_conserve_round(const float* in, float* out, long long n, cudaStream_t s);
 cudaError_t launch_conservation(const FluidDev& F, int reversed, double* partial, double* out, cudaStream_t s);
 
 }  // namespace glsm

@@ -239,6 +239,24 @@ int glsm_fluid_conservation(glsm_fluid f, double out[4]);
  * Results differ from the atomic form only by round-off.  Cost: one pass over
  * the box's markers per box cell and substep. */
 int glsm_fluid_set_deterministic(glsm_fluid f, int on);
+/* Rounding of FP16 population storage (extension; the reference stores FP32).
+ * mode 0 (default): each post-collision value rounds to nearest.  mode 1,
+ * conserving: each cell's 19 values are rounded so that the cell's summed mass
+ * and momentum rounding errors nearly cancel (round to nearest, then one
+ * greedy pass in which a value may take its other FP16 neighbour when that
+ * lowers the squared mass and momentum error).  mode 2: conserving on odd
+ * substeps, to nearest on even ones.  Round-to-nearest noise accumulates in
+ * long-wavelength modes that viscosity damps slowly; the conserving forms keep
+ * the long-horizon velocity error near that of a single rounding (mode 1) or
+ * halve the accumulation (mode 2), for about 390 more instructions per cell
+ * and conserving substep.  Needs FP16 storage; not while the system is in a
+ * batch. */
+int glsm_fluid_set_f16_rounding(glsm_fluid f, int mode);
+/* The conserving FP16 rounding on its own (verification aid, no counterpart in
+ * the reference): in and out hold n_cells x 19 scaled values ([cell][q], q in
+ * the D3Q19 order above) in host memory; out receives the float values of the
+ * chosen FP16 numbers.  At most 2^26 cells per call. */
+int glsm_f16_conserve_round(const float* in, float* out, size_t n_cells);
 /* nx, ny, nz, N, nsub, storage, device bytes, substeps done */
 int glsm_fluid_info(glsm_fluid f, int64_t out[8]);
 /* Fluid::stepVelocity(iter) with a CUDA event pair around each substep launch on

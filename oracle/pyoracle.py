@@ -219,3 +219,51 @@ def filament(un_norm, vn_norm, LX, LY, LZ, viso=0.15):
                 if r is not None:
                     out.append((xi + r[0], yi + r[1], float(zi)))
     return np.array(out, dtype=np.float64).reshape(-1, 3)
+
+
+# D3Q19 velocities in the reference's direction order (src/fluid.cu:202-215)
+D3Q19_C = np.array([[0, 0, 0], [1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1],
+                    [1, 1, 0], [-1, 1, 0], [-1, -1, 0], [1, -1, 0], [1, 0, 1], [-1, 0, 1], [-1, 0, -1],
+                    [1, 0, -1], [0, 1, 1], [0, 1, -1], [0, -1, -1], [0, -1, 1]])
+
+
+def conserve_round_f16(v):
+    """float32 restatement of the library's conserving FP16 rounding (FP16
+    storage option; the reference stores FP32, so this has no reference
+    counterpart).  v: (n, 19) float32 scaled post-collision values of n cells.
+    Every value is rounded to nearest FP16; then for q = 1..18 in order a value
+    moves one FP16 spacing towards its exact value when that lowers M^2 + |P|^2
+    (the cell's summed mass and momentum rounding errors so far).  Returns the
+    float32 values of the chosen FP16 numbers.  All arithmetic is float32 with
+    one rounding per operation, in the kernel's order."""
+    f32 = np.float32
+    v = np.asarray(v, dtype=f32)
+    h = v.astype(np.float16).astype(f32)
+    e = (v - h).astype(f32)
+    n = v.shape[0]
+    M = np.zeros(n, f32)
+    P = np.zeros((3, n), f32)
+    for q in range(19):
+        M = (M + e[:, q]).astype(f32)
+        for a in range(3):
+            c = D3Q19_C[q, a]
+            if c:
+                P[a] = (P[a] + e[:, q] if c > 0 else P[a] - e[:, q]).astype(f32)
+    for q in range(1, 19):
+        c = D3Q19_C[q]
+        bits = h[:, q].view(np.int32) & np.int32(0x7F800000)
+        ulp = np.maximum((bits - np.int32(10 << 23)).view(f32), f32(2.0 ** -24))
+        de = np.copysign(ulp, -e[:, q]).astype(f32)
+        t = M.copy()
+        for a in range(3):
+            if c[a]:
+                t = (t + P[a] if c[a] > 0 else t - P[a]).astype(f32)
+        k = f32(1 + int((c * c).sum()))
+        s = ((f32(2.0) * t).astype(f32) + (k * de).astype(f32)).astype(f32)
+        move = (de * s).astype(f32) < f32(0.0)
+        h[:, q] = np.where(move, (h[:, q] - de).astype(f32), h[:, q])
+        M = np.where(move, (M + de).astype(f32), M)
+        for a in range(3):
+            if c[a]:
+                P[a] = np.where(move, (P[a] + de if c[a] > 0 else P[a] - de).astype(f32), P[a])
+    return h

@@ -99,8 +99,8 @@ def test_deterministic_same_alone_and_in_batch(gpu):
 
 
 def test_deterministic_same_alone_and_in_a_mixed_batch(gpu):
-    """The batch launches its systems in groups (storage, x periodicity,
-    substep parity); one batch holding every kind, with systems that join with
+    """The batch launches its systems in groups (storage and FP16 rounding, x
+    periodicity, substep parity); one batch holding every kind, with systems that join with
     an odd substep count after running alone first, still reproduces each
     system alone bit for bit."""
     from glsm_fluid_3d_b200 import Batch, System
@@ -110,7 +110,9 @@ def test_deterministic_same_alone_and_in_a_mixed_batch(gpu):
              ((24, 20, 16), (5.75, 4.75, 3.75), "f16", (0, 0, 0), 1),
              ((18, 22, 20), (4.25, 5.75, 4.75), "bf16", (1, 0, 0), 0),
              ((22, 16, 18), (5.25, 3.75, 4.25), "f32", (1, 0, 1), 1),
-             ((16, 24, 20), (3.75, 5.25, 4.75), "f16", (1, 0, 0), 2)]
+             ((16, 24, 20), (3.75, 5.25, 4.75), "f16", (1, 0, 0), 2),
+             ((20, 20, 18), (4.75, 4.75, 4.25), "f16c", (0, 0, 0), 1),
+             ((18, 20, 22), (4.25, 4.75, 5.25), "f16c2", (1, 0, 0), 0)]
 
     def make(dims, pos, storage, periodic, seed):
         s = System(*dims, nsub=3, storage=storage, deterministic=True)

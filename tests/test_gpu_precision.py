@@ -2,7 +2,8 @@
 moments) against the FP64 oracle on the golden cases.
 
 FP16 stores the deviations scaled by 2^20 (its normal range then covers
-deviations from 6e-11 to 0.06 with 11-bit precision); BF16 stores them
+deviations from 6e-11 to 0.06 with 11-bit precision), rounded to nearest or
+("f16c") with the mass- and momentum-conserving rounding; BF16 stores them
 unscaled with 8-bit precision.  The tolerances below are relative L2 errors.
 """
 import numpy as np
@@ -18,9 +19,10 @@ TOL = {
     "f16": {"u": 2e-3, "Ul": 2e-3, "pop": 1e-5, "c1": 1e-4, "rn": 1e-7, "um": 1e-7},
     "bf16": {"u": 3e-2, "Ul": 3e-2, "pop": 1e-4, "c1": 1e-3, "rn": 1e-6, "um": 1e-6},
 }
+TOL["f16c"] = TOL["f16c2"] = TOL["f16"]  # FP16 storage with the conserving rounding
 
 
-@pytest.mark.parametrize("storage", ["f16", "bf16"])
+@pytest.mark.parametrize("storage", ["f16", "f16c", "f16c2", "bf16"])
 @pytest.mark.parametrize("case", list(CASES))
 def test_low_precision_storage_vs_oracle(gpu, storage, case):
     from glsm_fluid_3d_b200 import System
