@@ -27,7 +27,8 @@ import numpy as np
 
 from ._lib import FluidDesc, GlsmError, check, lib
 
-__all__ = ["Gel", "Coupler", "Fluid", "System", "Batch", "GlsmError", "STORAGE", "lib", "copy_bandwidth"]
+__all__ = ["Gel", "Coupler", "Fluid", "System", "Batch", "GlsmError", "STORAGE", "lib", "copy_bandwidth",
+           "l2_reset_persisting"]
 
 STORAGE = {"f32": 0, "fp32": 0, "f16": 1, "fp16": 1, "bf16": 2, "f16c": 1, "f16c2": 1}
 # FP16 rounding modes (glsm_fluid_set_f16_rounding); storage "f16c" is FP16
@@ -43,6 +44,12 @@ GEL_FIELDS = {
 }
 FLUID_FIELDS = {"pop": 0, "rho": 1, "u": 2, "c1": 3}
 MARKER_FIELDS = {"lag": 0, "Ul": 1, "Vl": 2, "Fdrag": 3, "Frep": 4, "Cl": 5, "Dl": 6, "Sl": 7}
+
+
+def l2_reset_persisting():
+    """Turn every persisting L2 line back into a normal one (glsm_l2_reset_persisting);
+    call with the GPU idle, before flushing L2 between timed steps."""
+    check(lib().glsm_l2_reset_persisting(), "l2_reset_persisting")
 
 
 def copy_bandwidth(nbytes: int, reps: int) -> float:
@@ -266,6 +273,11 @@ class Fluid:
             self.set_deterministic(True)
         if rounding:
             self.set_f16_rounding(rounding)
+
+    def set_l2_persisting(self, on=True):
+        """Keep the population array in the persisting part of L2 across the
+        substeps (on by default; glsm_fluid_set_l2_persisting)."""
+        check(self.L.glsm_fluid_set_l2_persisting(self.h, 1 if on else 0), "set_l2_persisting")
 
     def set_f16_rounding(self, mode="conserving"):
         """Rounding of FP16 storage: "nearest", "conserving" (each cell's

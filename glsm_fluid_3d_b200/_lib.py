@@ -86,6 +86,8 @@ def lib():
         "glsm_batch_run": [vp, i],
         "glsm_batch_sync": [vp],
         "glsm_fluid_set_f16_rounding": [vp, i],
+        "glsm_fluid_set_l2_persisting": [vp, i],
+        "glsm_l2_reset_persisting": [],
         "glsm_f16_conserve_round": [vp, vp, ctypes.c_size_t],
     }
     for name, args in sig.items():

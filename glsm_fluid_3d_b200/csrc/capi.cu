@@ -87,6 +87,9 @@ struct glsm_fluid_s {
     int lbm_ctas = 0;            // resident CTAs of the persistent substep kernel (odd substeps)
     int lbm_ctas_even = 0;       // the same for even substeps
     int staged_ctas = 0;         // resident CTAs of the staged substep kernel (0: not used)
+    int l2_on = 1;               // keep the population array L2-persisting (glsm_fluid_set_l2_persisting)
+    unsigned long long l2_bytes = 0;  // access-policy window of the substep launches (0: none)
+    float l2_hit = 0.f;
     double* d_cons = nullptr;    // conservation partial sums (kConsBlocks x 4) and result (4)
     struct glsm_batch_s* batch = nullptr;  // batch this system belongs to
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -841,7 +844,43 @@ static StepArgs step_args(glsm_fluid f, int k, int iter_arg) {
     a.lbm_ctas = f->lbm_ctas;
     a.lbm_ctas_even = f->lbm_ctas_even;
     a.staged_ctas = f->staged_ctas;
+    a.l2_bytes = f->l2_bytes;
+    a.l2_hit = f->l2_hit;
     return a;
+}
+
+// L2 residency of the population array (101^3: 78 MB FP32, 39 MB FP16 of the
+// 126 MB L2).  The substep launches carry an access-policy window that marks
+// the array persisting, so the array stays in L2 across the substeps of an
+// iteration instead of competing with the streams of u, the forces and the
+// concentration.  The persisting set-aside is a limit of the CUDA context: it
+// grows to the largest array among the process's fluids, capped by the
+// device's maximum, and ends with the process.  Must not run during a capture.
+static void l2_window(glsm_fluid f) {
+    f->l2_bytes = 0;
+    f->l2_hit = 0.f;
+    if (!f->l2_on) return;
+    int dev = 0, max_persist = 0, max_window = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess ||
+        max_persist <= 0 || max_window <= 0) {
+        cudaGetLastError();
+        return;
+    }
+    const size_t esz = (f->F.storage == GLSM_STORE_F32) ? 4 : 2;
+    const size_t bytes = std::min((size_t)19 * (size_t)f->F.S * esz, (size_t)max_window);
+    size_t cur = 0;
+    cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+    const size_t want = std::min(bytes, (size_t)max_persist);
+    if (cur < want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
+    if (cur == 0) return;
+    f->l2_bytes = bytes;
+    f->l2_hit = std::min(1.0f, (float)cur / (float)bytes);
 }
 
 int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out) {
@@ -937,6 +976,7 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     }
     f->c = c;
     c->fluid = f;
+    l2_window(f);
     // the gels' gather now knows the lattice
     *out = f;
     return GLSM_OK;
@@ -968,6 +1008,27 @@ int glsm_fluid_set_deterministic(glsm_fluid f, int on) {
                 cudaGraphExecDestroy(g);
                 g = nullptr;
             }
+    return GLSM_OK;
+}
+
+int glsm_fluid_set_l2_persisting(glsm_fluid f, int on) {
+    if (!f) return fail(GLSM_ERR_ARG, "null fluid");
+    if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
+    CK(cudaStreamSynchronize(f->c->stream));
+    f->l2_on = on ? 1 : 0;
+    l2_window(f);
+    // the captured iteration graphs hold the old launch attributes
+    for (auto& row : f->graph)
+        for (auto& g : row)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    return GLSM_OK;
+}
+
+int glsm_l2_reset_persisting(void) {
+    CK(cudaCtxResetPersistingL2Cache());
     return GLSM_OK;
 }
 

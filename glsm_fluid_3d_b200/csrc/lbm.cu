@@ -1552,16 +1552,28 @@ cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
     // marker boxes its prologue reads, so it is launched plainly.  GLSM_NO_PDL=1
     // launches every substep plainly.
     static const bool no_pdl = getenv("GLSM_NO_PDL") != nullptr;
-    cudaLaunchAttribute attr[1];
+    cudaLaunchAttribute attr[2];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = (no_pdl || a.k == 0) ? 0 : 1;
+    int n_attr = 1;
+    if (a.l2_bytes > 0) {
+        // the population array stays in the persisting part of L2 across the
+        // substeps of an iteration
+        attr[1].id = cudaLaunchAttributeAccessPolicyWindow;
+        attr[1].val.accessPolicyWindow.base_ptr = a.F.pop;
+        attr[1].val.accessPolicyWindow.num_bytes = (size_t)a.l2_bytes;
+        attr[1].val.accessPolicyWindow.hitRatio = a.l2_hit;
+        attr[1].val.accessPolicyWindow.hitProp = cudaAccessPropertyPersisting;
+        attr[1].val.accessPolicyWindow.missProp = cudaAccessPropertyStreaming;
+        n_attr = 2;
+    }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = grid;
     cfg.blockDim = block;
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cfg.attrs = attr;
-    cfg.numAttrs = 1;
+    cfg.numAttrs = n_attr;
 #define GLSM_SUB2(ST, DET)                                                     \
     if (parity && a.F.per[0])                                                  \
         return cudaLaunchKernelEx(&cfg, lbm_substep_kernel<ST, 1, 1, DET>, a); \

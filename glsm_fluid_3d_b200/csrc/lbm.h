@@ -21,6 +21,8 @@ struct StepArgs {
     int lbm_ctas;        // persistent CTAs per odd-substep launch (0: one per ticket)
     int lbm_ctas_even;   // persistent CTAs per even-substep launch (0: one per ticket)
     int staged_ctas;     // > 0: the shared-memory staged kernel with this many CTAs
+    float l2_hit;        // > 0: substep launches mark the first l2_bytes of the population
+    unsigned long long l2_bytes;  // array L2-persisting with this hit ratio
 };
 
 struct ConcArgs {

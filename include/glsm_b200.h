@@ -252,6 +252,18 @@ int glsm_fluid_set_deterministic(glsm_fluid f, int on);
  * and conserving substep.  Needs FP16 storage; not while the system is in a
  * batch. */
 int glsm_fluid_set_f16_rounding(glsm_fluid f, int mode);
+/* L2 residency of the population array (extension; the reference leaves L2 to
+ * the hardware).  on = 1 (the default from glsm_fluid_create): the substep
+ * launches carry an access-policy window that marks the array persisting, so a
+ * 101^3 array (78 MB FP32) stays in the 126 MB L2 across the substeps of an
+ * iteration.  The persisting set-aside is a limit of the process's CUDA
+ * context (grown to the largest array of its fluids, at most the device's
+ * maximum); it ends with the process.  Not while the system is in a batch. */
+int glsm_fluid_set_l2_persisting(glsm_fluid f, int on);
+/* Turns every persisting L2 line of the context back into a normal one
+ * (cudaCtxResetPersistingL2Cache): a benchmark calls it, with the stream idle,
+ * before it flushes L2 between timed steps. */
+int glsm_l2_reset_persisting(void);
 /* The conserving FP16 rounding on its own (verification aid, no counterpart in
  * the reference): in and out hold n_cells x 19 scaled values ([cell][q], q in
  * the D3Q19 order above) in host memory; out receives the float values of the

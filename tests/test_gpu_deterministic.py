@@ -148,3 +148,23 @@ def test_deterministic_same_alone_and_in_a_mixed_batch(gpu):
         b.remove(s.fluid)
         s.close()
     b.close()
+
+
+def test_l2_persisting_window_changes_no_result(gpu):
+    """The L2 access-policy window of the substep launches (on by default) only
+    steers caching: with deterministic spreads the results are bit-identical
+    with it switched off, and releasing the persisting lines between runs
+    changes nothing either."""
+    from glsm_fluid_3d_b200 import System, l2_reset_persisting
+
+    outs = []
+    for on in (True, False):
+        sim = build(System, "pair", deterministic=True)
+        sim.fluid.set_l2_persisting(on)
+        sim.run(0, CASES["pair"]["iters"] // 2)
+        l2_reset_persisting()
+        sim.run(CASES["pair"]["iters"] // 2, CASES["pair"]["iters"] - CASES["pair"]["iters"] // 2)
+        outs.append(collect(sim, "pair"))
+        sim.close()
+    diff = [k for k in outs[0] if not np.array_equal(outs[0][k], outs[1][k])]
+    assert not diff, diff
