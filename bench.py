@@ -85,6 +85,8 @@ def parse():
                    help="D: 101^3 two gels (default); S: 48^3 one gel; P: 256^3 eight gels; L: 384x384x192 rods")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-l2-persisting", action="store_true",
+                   help="leave the population array's L2 access-policy window off")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
     return p.parse_args()
 
@@ -273,6 +275,7 @@ def run_ours(args, world, rank, local):
     l2 = copy_bandwidth(L2_PROBE_BYTES, L2_PROBE_REPS)
     s = make_system(args.storage)
     fluid = s.fluid
+    fluid.set_l2_persisting(not args.no_l2_persisting)  # one system alone on the GPU
     stream = torch.cuda.ExternalStream(s.coupler.stream())
     flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     clocks = Clocks(local)
@@ -402,7 +405,8 @@ def run_ours(args, world, rank, local):
         "metric": "coupled MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(t_ms / K, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": args.storage, "data": "synthetic (seeded gel chemistry noise, fluid at rest)",
-        "config": workload_desc(args.storage), "roofline": roof, "cpu_baseline": base, "e2e": e2e,
+        "config": dict(workload_desc(args.storage), l2_persisting=not args.no_l2_persisting),
+        "roofline": roof, "cpu_baseline": base, "e2e": e2e,
         "clocks": clk, "gpu_launches": launches_per_step * K,
     }
     s.close()

@@ -276,7 +276,8 @@ class Fluid:
 
     def set_l2_persisting(self, on=True):
         """Keep the population array in the persisting part of L2 across the
-        substeps (on by default; glsm_fluid_set_l2_persisting)."""
+        substeps (off by default; for one system alone on the GPU;
+        glsm_fluid_set_l2_persisting)."""
         check(self.L.glsm_fluid_set_l2_persisting(self.h, 1 if on else 0), "set_l2_persisting")
 
     def set_f16_rounding(self, mode="conserving"):

@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -87,7 +88,7 @@ struct glsm_fluid_s {
     int lbm_ctas = 0;            // resident CTAs of the persistent substep kernel (odd substeps)
     int lbm_ctas_even = 0;       // the same for even substeps
     int staged_ctas = 0;         // resident CTAs of the staged substep kernel (0: not used)
-    int l2_on = 1;               // keep the population array L2-persisting (glsm_fluid_set_l2_persisting)
+    int l2_on = 0;               // keep the population array L2-persisting (glsm_fluid_set_l2_persisting)
     unsigned long long l2_bytes = 0;  // access-policy window of the substep launches (0: none)
     float l2_hit = 0.f;
     double* d_cons = nullptr;    // conservation partial sums (kConsBlocks x 4) and result (4)
@@ -850,37 +851,57 @@ static StepArgs step_args(glsm_fluid f, int k, int iter_arg) {
 }
 
 // L2 residency of the population array (101^3: 78 MB FP32, 39 MB FP16 of the
-// 126 MB L2).  The substep launches carry an access-policy window that marks
-// the array persisting, so the array stays in L2 across the substeps of an
-// iteration instead of competing with the streams of u, the forces and the
-// concentration.  The persisting set-aside is a limit of the CUDA context: it
-// grows to the largest array among the process's fluids, capped by the
-// device's maximum, and ends with the process.  Must not run during a capture.
-static void l2_window(glsm_fluid f) {
-    f->l2_bytes = 0;
-    f->l2_hit = 0.f;
-    if (!f->l2_on) return;
-    int dev = 0, max_persist = 0, max_window = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev) != cudaSuccess ||
-        max_persist <= 0 || max_window <= 0) {
-        cudaGetLastError();
-        return;
-    }
-    const size_t esz = (f->F.storage == GLSM_STORE_F32) ? 4 : 2;
-    const size_t bytes = std::min((size_t)19 * (size_t)f->F.S * esz, (size_t)max_window);
+// 126 MB L2), opt-in per fluid.  The substep launches then carry an
+// access-policy window that marks the array persisting, so it stays in L2
+// across the substeps of an iteration.  The persisting set-aside is a limit of
+// the CUDA context, and L2 it reserves is lost to every access outside a window
+// (a batch's launches, other fluids, the caller's own kernels): it is sized to
+// the largest window of the fluids that use one and released (set to zero,
+// persisting lines reset) when the last of them stops.  Must not run during a
+// capture.
+static std::mutex g_l2_mu;
+static std::vector<glsm_fluid_s*> g_l2_users;
+
+static void l2_setaside_locked() {
+    size_t want = 0;
+    for (auto* u : g_l2_users) want = std::max(want, (size_t)u->l2_bytes);
+    int dev = 0, max_persist = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev);
+    want = std::min(want, (size_t)std::max(max_persist, 0));
+    if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) cudaGetLastError();
+    if (want == 0 && cudaCtxResetPersistingL2Cache() != cudaSuccess) cudaGetLastError();
     size_t cur = 0;
     cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
-    const size_t want = std::min(bytes, (size_t)max_persist);
-    if (cur < want && cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) {
-        cudaGetLastError();
-        return;
+    for (auto* u : g_l2_users) u->l2_hit = cur ? std::min(1.0f, (float)cur / (float)u->l2_bytes) : 0.f;
+}
+
+// enables (on) or disables the window of f and resizes the set-aside
+static void l2_window(glsm_fluid f, int on) {
+    std::lock_guard<std::mutex> lock(g_l2_mu);
+    auto it = std::find(g_l2_users.begin(), g_l2_users.end(), f);
+    const bool was = it != g_l2_users.end();
+    if (was) g_l2_users.erase(it);
+    f->l2_on = 0;
+    f->l2_bytes = 0;
+    f->l2_hit = 0.f;
+    int dev = 0, max_window = 0;
+    if (on && cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev) == cudaSuccess &&
+        max_window > 0) {
+        const size_t esz = (f->F.storage == GLSM_STORE_F32) ? 4 : 2;
+        f->l2_on = 1;
+        f->l2_bytes = std::min((size_t)19 * (size_t)f->F.S * esz, (size_t)max_window);
+        g_l2_users.push_back(f);
     }
-    cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
-    if (cur == 0) return;
-    f->l2_bytes = bytes;
-    f->l2_hit = std::min(1.0f, (float)cur / (float)bytes);
+    cudaGetLastError();
+    if (was || f->l2_on) l2_setaside_locked();
+    if (f->l2_on && f->l2_hit <= 0.f) {  // no set-aside could be had
+        g_l2_users.pop_back();
+        f->l2_on = 0;
+        f->l2_bytes = 0;
+        l2_setaside_locked();
+    }
 }
 
 int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out) {
@@ -976,7 +997,6 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     }
     f->c = c;
     c->fluid = f;
-    l2_window(f);
     // the gels' gather now knows the lattice
     *out = f;
     return GLSM_OK;
@@ -986,6 +1006,7 @@ int glsm_fluid_destroy(glsm_fluid f) {
     if (!f) return GLSM_OK;
     if (f->batch) return fail(GLSM_ERR_STATE, "remove the system from its batch first");
     cudaStreamSynchronize(f->c->stream);
+    if (f->l2_on) l2_window(f, 0);
     for (auto& row : f->graph)
         for (auto& g : row)
             if (g) cudaGraphExecDestroy(g);
@@ -1015,8 +1036,7 @@ int glsm_fluid_set_l2_persisting(glsm_fluid f, int on) {
     if (!f) return fail(GLSM_ERR_ARG, "null fluid");
     if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
     CK(cudaStreamSynchronize(f->c->stream));
-    f->l2_on = on ? 1 : 0;
-    l2_window(f);
+    l2_window(f, on);
     // the captured iteration graphs hold the old launch attributes
     for (auto& row : f->graph)
         for (auto& g : row)
@@ -1661,6 +1681,17 @@ int glsm_batch_add(glsm_batch b, glsm_fluid f, int iter0, int n_iters) {
     if (!b->sys.empty() && f->F.nsub != b->nsub) return fail(GLSM_ERR_ARG, "all systems of a batch need the same nsub");
     CK(cudaStreamSynchronize(f->c->stream));
     CK(cudaStreamSynchronize(b->stream));
+    // batched launches carry no access-policy window: a joining system gives
+    // up its L2 set-aside
+    if (f->l2_on) {
+        l2_window(f, 0);
+        for (auto& row : f->graph)
+            for (auto& g : row)
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
+    }
     if (b->sys.empty()) b->nsub = f->F.nsub;
     set_iter_kernel<<<1, 1, 0, b->stream>>>(f->c->d_ctl, iter0);
     CK(cudaGetLastError());

@@ -253,12 +253,15 @@ int glsm_fluid_set_deterministic(glsm_fluid f, int on);
  * batch. */
 int glsm_fluid_set_f16_rounding(glsm_fluid f, int mode);
 /* L2 residency of the population array (extension; the reference leaves L2 to
- * the hardware).  on = 1 (the default from glsm_fluid_create): the substep
- * launches carry an access-policy window that marks the array persisting, so a
- * 101^3 array (78 MB FP32) stays in the 126 MB L2 across the substeps of an
- * iteration.  The persisting set-aside is a limit of the process's CUDA
- * context (grown to the largest array of its fluids, at most the device's
- * maximum); it ends with the process.  Not while the system is in a batch. */
+ * the hardware).  on = 1 (off by default): the substep launches carry an
+ * access-policy window that marks the array persisting, so a 101^3 array
+ * (78 MB FP32) stays in the 126 MB L2 across the substeps of an iteration.
+ * The persisting set-aside is a limit of the process's CUDA context, and the
+ * L2 it reserves is lost to every access outside a window (other fluids, a
+ * batch, the caller's kernels): it is sized to the largest window in use and
+ * released when the last fluid using one turns it off, is destroyed or joins a
+ * batch (which turns it off).  For one system alone on the GPU.  Not while the
+ * system is in a batch. */
 int glsm_fluid_set_l2_persisting(glsm_fluid f, int on);
 /* Turns every persisting L2 line of the context back into a normal one
  * (cudaCtxResetPersistingL2Cache): a benchmark calls it, with the stream idle,
