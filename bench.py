@@ -405,7 +405,7 @@ def run_ours(args, world, rank, local):
         "metric": "coupled MLUPS", "value": round(value, 1), "unit": "MLUPS", "n_gpus": world, "steps": K,
         "warmup": args.warmup, "ms_per_step": round(t_ms / K, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": args.storage, "data": "synthetic (seeded gel chemistry noise, fluid at rest)",
-        "config": dict(workload_desc(args.storage), l2_persisting=not args.no_l2_persisting),
+        "config": workload_desc(args.storage), "l2_persisting": not args.no_l2_persisting,
         "roofline": roof, "cpu_baseline": base, "e2e": e2e,
         "clocks": clk, "gpu_launches": launches_per_step * K,
     }
