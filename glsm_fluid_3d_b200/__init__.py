@@ -28,7 +28,7 @@ import numpy as np
 from ._lib import FluidDesc, GlsmError, check, lib
 
 __all__ = ["Gel", "Coupler", "Fluid", "System", "Batch", "GlsmError", "STORAGE", "lib", "copy_bandwidth",
-           "l2_reset_persisting"]
+           "l2_reset_persisting", "l2_persisting_setaside"]
 
 STORAGE = {"f32": 0, "fp32": 0, "f16": 1, "fp16": 1, "bf16": 2, "f16c": 1, "f16c2": 1}
 # FP16 rounding modes (glsm_fluid_set_f16_rounding); storage "f16c" is FP16
@@ -50,6 +50,13 @@ def l2_reset_persisting():
     """Turn every persisting L2 line back into a normal one (glsm_l2_reset_persisting);
     call with the GPU idle, before flushing L2 between timed steps."""
     check(lib().glsm_l2_reset_persisting(), "l2_reset_persisting")
+
+
+def l2_persisting_setaside() -> int:
+    """The context's persisting L2 set-aside in bytes (glsm_l2_persisting_setaside)."""
+    out = ctypes.c_size_t(0)
+    check(lib().glsm_l2_persisting_setaside(ctypes.byref(out)), "l2_persisting_setaside")
+    return out.value
 
 
 def copy_bandwidth(nbytes: int, reps: int) -> float:

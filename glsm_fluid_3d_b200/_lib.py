@@ -88,6 +88,7 @@ def lib():
         "glsm_fluid_set_f16_rounding": [vp, i],
         "glsm_fluid_set_l2_persisting": [vp, i],
         "glsm_l2_reset_persisting": [],
+        "glsm_l2_persisting_setaside": [P(ctypes.c_size_t)],
         "glsm_f16_conserve_round": [vp, vp, ctypes.c_size_t],
     }
     for name, args in sig.items():

@@ -1052,6 +1052,12 @@ int glsm_l2_reset_persisting(void) {
     return GLSM_OK;
 }
 
+int glsm_l2_persisting_setaside(size_t* bytes) {
+    if (!bytes) return fail(GLSM_ERR_ARG, "null argument");
+    CK(cudaDeviceGetLimit(bytes, cudaLimitPersistingL2CacheSize));
+    return GLSM_OK;
+}
+
 int glsm_fluid_set_f16_rounding(glsm_fluid f, int mode) {
     if (!f) return fail(GLSM_ERR_ARG, "null fluid");
     if (mode < 0 || mode > 2)

@@ -267,6 +267,9 @@ int glsm_fluid_set_l2_persisting(glsm_fluid f, int on);
  * (cudaCtxResetPersistingL2Cache): a benchmark calls it, with the stream idle,
  * before it flushes L2 between timed steps. */
 int glsm_l2_reset_persisting(void);
+/* The context's current persisting L2 set-aside in bytes (0 when no fluid keeps
+ * its populations L2-persisting). */
+int glsm_l2_persisting_setaside(size_t* bytes);
 /* The conserving FP16 rounding on its own (verification aid, no counterpart in
  * the reference): in and out hold n_cells x 19 scaled values ([cell][q], q in
  * the D3Q19 order above) in host memory; out receives the float values of the

@@ -168,3 +168,41 @@ def test_l2_persisting_window_changes_no_result(gpu):
         sim.close()
     diff = [k for k in outs[0] if not np.array_equal(outs[0][k], outs[1][k])]
     assert not diff, diff
+
+
+def test_l2_setaside_follows_the_fluids_that_use_it(gpu):
+    """The persisting L2 set-aside exists only while a fluid keeps its
+    populations L2-persisting: sized to the largest such array, released when
+    the last one turns the window off, is destroyed or joins a batch."""
+    from glsm_fluid_3d_b200 import Batch, System, l2_persisting_setaside
+
+    def make(dims, storage):
+        s = System(*dims, nsub=3, storage=storage)
+        s.add_gel((3, 3, 3), (4.75, 4.75, 4.75), 1, 1)
+        s.set_params(beta=1.0, ramp_steps=0.0)
+        s.finalize()
+        return s
+
+    assert l2_persisting_setaside() == 0
+    a = make((64, 64, 64), "f32")
+    b = make((24, 24, 24), "f16")
+    assert l2_persisting_setaside() == 0  # off by default
+    a.fluid.set_l2_persisting(True)
+    big = l2_persisting_setaside()
+    assert big > 0
+    b.fluid.set_l2_persisting(True)
+    assert l2_persisting_setaside() == big  # the largest window in use
+    a.fluid.set_l2_persisting(False)
+    small = l2_persisting_setaside()
+    assert 0 < small < big
+    a.fluid.set_l2_persisting(True)
+    a.close()  # destroying a user releases its share
+    assert l2_persisting_setaside() == small
+    batch = Batch()
+    batch.add(b.fluid, 0, 2)  # joining a batch turns the window off
+    assert l2_persisting_setaside() == 0
+    batch.run(2)
+    batch.sync()
+    batch.remove(b.fluid)
+    batch.close()
+    b.close()
