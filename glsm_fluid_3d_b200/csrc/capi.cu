@@ -827,7 +827,10 @@ int glsm_fluid_desc_default(glsm_fluid_desc* d, int nx, int ny, int nz) {
 
 __global__ void u_rest_kernel(float4* u, long long N);
 
-static StepArgs step_args(glsm_fluid f, int k, int iter_arg) {
+// last-wave half tiles of the substep launches, in waves of the resident CTAs
+constexpr int kTailWaves = 1;
+
+static StepArgs step_args(glsm_fluid f, int k, int iter_arg, bool tail = true) {
     StepArgs a{};
     a.F = f->F;
     a.Mk = f->c->mk;
@@ -841,7 +844,17 @@ static StepArgs step_args(glsm_fluid f, int k, int iter_arg) {
     a.last = (k == f->F.nsub - 1);
     a.div_nx = make_fastdiv((unsigned)f->F.nx);
     a.div_nxy = make_fastdiv((unsigned)(f->F.nx * f->F.ny));
-    a.n_tiles = (int)((f->F.N + kTileCells - 1) / kTileCells);
+    // full tiles, then half tiles for the last kTailWaves waves of resident
+    // CTAs (none in a batch, whose launches mix systems, nor for the staged
+    // kernel, which stages whole tiles)
+    const long long N = f->F.N;
+    const long long tail_cells = (tail && f->staged_ctas == 0)
+                                     ? (long long)kTailWaves * std::max(f->lbm_ctas, 1) * (kTileCells / 2)
+                                     : 0;
+    const long long big = std::max(0LL, (N - tail_cells) / kTileCells);
+    a.big_tiles = (int)big;
+    a.n_tiles = (int)(big + (N - big * kTileCells + kTileCells / 2 - 1) / (kTileCells / 2));
+    if (tail_cells == 0) a.big_tiles = a.n_tiles = (int)((N + kTileCells - 1) / kTileCells);
     a.lbm_ctas = f->lbm_ctas;
     a.lbm_ctas_even = f->lbm_ctas_even;
     a.staged_ctas = f->staged_ctas;
@@ -1508,7 +1521,7 @@ static int batch_rebuild(glsm_batch_s* b) {
         gibm_off.push_back(0);
         gtile_off.push_back(0);
         for (int i : groups[gi].members) {
-            const StepArgs a = step_args(b->sys[i], 0, -1);
+            const StepArgs a = step_args(b->sys[i], 0, -1, false);
             members.push_back(i);
             gibm_off.push_back(io += a.n_ibm);
             gtile_off.push_back(to += a.n_tiles);
@@ -1518,7 +1531,7 @@ static int batch_rebuild(glsm_batch_s* b) {
     for (int i = 0; i < n; i++) {
         glsm_fluid_s* f = b->sys[i];
         glsm_coupler c = f->c;
-        StepArgs a = step_args(f, 0, -1);
+        StepArgs a = step_args(f, 0, -1, false);
         hs[i].step = a;
         hs[i].conc = ConcArgs{f->F, c->mk, c->d_ctl, (int)c->gels.size(), 0, 0, make_fastdiv((unsigned)f->F.nx),
                               make_fastdiv((unsigned)(f->F.nx * f->F.ny))};

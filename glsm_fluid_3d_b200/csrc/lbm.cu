@@ -701,13 +701,26 @@ struct TileSlot {
     int g[kMaxBoxes];  // gel index of each box
 };
 
+// Cell range of lattice tile `tile`: tiles of kTileCells cells, then, for
+// the last wave of a launch, tiles of half that size.  A persistent launch
+// ends when its slowest CTA finishes its last tile, so finer tiles at the end
+// shorten the time the other CTAs wait, while the bulk keeps the per-tile
+// overhead of full tiles.  Half tiles start at even cells, as the paired FP16
+// even substep needs.
+__device__ __forceinline__ void tile_range(const StepArgs& a, unsigned tile, unsigned& c0, unsigned& c1) {
+    const unsigned big = (unsigned)a.big_tiles;
+    const bool full = tile < big;
+    c0 = full ? tile * kTileCells : big * kTileCells + (tile - big) * (kTileCells / 2);
+    c1 = min(c0 + (full ? kTileCells : kTileCells / 2) - 1, (unsigned)a.F.N - 1);
+}
+
 __device__ __forceinline__ void prepare_slot(const StepArgs& a, unsigned t, TileSlot& sl) {
     const unsigned lane = threadIdx.x & 31;
     int nb = 0;
     if (t >= (unsigned)a.n_ibm && t < (unsigned)(a.n_ibm + a.n_tiles)) {
         const FluidDev& F = a.F;
-        const unsigned c0 = (t - a.n_ibm) * kTileCells;
-        const unsigned c1 = min(c0 + kTileCells - 1, (unsigned)F.N - 1);
+        unsigned c0, c1;
+        tile_range(a, t - a.n_ibm, c0, c1);
         const TileExt ext = tile_extent(c0, c1, F.nx, F.ny, a.div_nx, a.div_nxy);
         for (int j0 = 0; j0 < a.n_boxes; j0 += 32) {
             const int j = j0 + (int)lane;
@@ -791,13 +804,12 @@ __device__ __forceinline__ bool in_boxes(const StepArgs& a, const TileSlot& sl, 
     return inb;
 }
 
-// a lattice tile of kTileCells consecutive cells, kCellsPerThread per thread:
-// adjacent pairs on even substeps of FP16 storage, else cells kTile apart
+// a lattice tile of consecutive cells (tile_range), up to kCellsPerThread per
+// thread: adjacent pairs on even substeps of FP16 storage, else cells kTile apart
 template <int ST, int PARITY, int PERX, bool PAIR = false, bool DET = false>
 __device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const TileSlot& sl) {
-    const FluidDev& F = a.F;
-    const unsigned c0 = tile * kTileCells;
-    const unsigned c1 = min(c0 + kTileCells - 1, (unsigned)F.N - 1);
+    unsigned c0, c1;
+    tile_range(a, tile, c0, c1);
     const int nb = sl.nb;
     if (nb > 0) wait_ibm(a);
     if constexpr (PAIR && PARITY == 0 && (ST == kStoreF16 || ST == kStoreF16C) && kCellsPerThread == 2) {
@@ -1188,8 +1200,8 @@ __device__ void prepare_batch_slot(const BatchLaunch& L, unsigned t, BatchSlot& 
         }
         if (!ibm) {
             const StepArgs& a = sys.step;
-            const unsigned c0 = local * kTileCells;
-            const unsigned c1 = min(c0 + kTileCells - 1, (unsigned)a.F.N - 1);
+            unsigned c0, c1;
+            tile_range(a, local, c0, c1);
             const TileExt ext = tile_extent(c0, c1, a.F.nx, a.F.ny, a.div_nx, a.div_nxy);
             for (int j0 = 0; j0 < a.n_boxes; j0 += 32) {
                 const int j = j0 + (int)lane;

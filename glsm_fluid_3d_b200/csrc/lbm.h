@@ -17,7 +17,8 @@ struct StepArgs {
     int k;               // substep index within the iteration
     int last;            // k == nsub - 1: write u for every cell
     FastDiv div_nx, div_nxy;
-    int n_tiles;         // lattice tiles of kTileCells cells
+    int n_tiles;         // lattice tiles
+    int big_tiles;       // tiles [0, big_tiles) hold kTileCells cells, the rest kTileCells / 2
     int lbm_ctas;        // persistent CTAs per odd-substep launch (0: one per ticket)
     int lbm_ctas_even;   // persistent CTAs per even-substep launch (0: one per ticket)
     int staged_ctas;     // > 0: the shared-memory staged kernel with this many CTAs
