@@ -898,13 +898,17 @@ static void l2_window(glsm_fluid f, int on) {
     f->l2_on = 0;
     f->l2_bytes = 0;
     f->l2_hit = 0.f;
-    int dev = 0, max_window = 0;
+    int dev = 0, max_window = 0, max_persist = 0;
+    const size_t esz = (f->F.storage == GLSM_STORE_F32) ? 4 : 2;
+    const size_t bytes = (size_t)19 * (size_t)f->F.S * esz;
+    // only an array that fits in the set-aside can stay resident; a larger
+    // one would reserve L2 without the benefit
     if (on && cudaGetDevice(&dev) == cudaSuccess &&
         cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev) == cudaSuccess &&
-        max_window > 0) {
-        const size_t esz = (f->F.storage == GLSM_STORE_F32) ? 4 : 2;
+        cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev) == cudaSuccess &&
+        bytes <= (size_t)std::max(max_window, 0) && bytes <= (size_t)std::max(max_persist, 0)) {
         f->l2_on = 1;
-        f->l2_bytes = std::min((size_t)19 * (size_t)f->F.S * esz, (size_t)max_window);
+        f->l2_bytes = bytes;
         g_l2_users.push_back(f);
     }
     cudaGetLastError();

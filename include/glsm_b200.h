@@ -260,8 +260,10 @@ int glsm_fluid_set_f16_rounding(glsm_fluid f, int mode);
  * L2 it reserves is lost to every access outside a window (other fluids, a
  * batch, the caller's kernels): it is sized to the largest window in use and
  * released when the last fluid using one turns it off, is destroyed or joins a
- * batch (which turns it off).  For one system alone on the GPU.  Not while the
- * system is in a batch. */
+ * batch (which turns it off).  For one system alone on the GPU whose array
+ * fits in the device's largest set-aside (82.9 MB on a B200: FP32 up to ~103^3
+ * cells, FP16 up to ~130^3); for a larger array the call leaves the window off.
+ * Not while the system is in a batch. */
 int glsm_fluid_set_l2_persisting(glsm_fluid f, int on);
 /* Turns every persisting L2 line of the context back into a normal one
  * (cudaCtxResetPersistingL2Cache): a benchmark calls it, with the stream idle,
