@@ -492,10 +492,11 @@ __device__ __forceinline__ void conserve_round(float (&d)[19]) {
         if (cx) t = cx > 0 ? __fadd_rn(t, Px) : __fsub_rn(t, Px);
         if (cy) t = cy > 0 ? __fadd_rn(t, Py) : __fsub_rn(t, Py);
         if (cz) t = cz > 0 ? __fadd_rn(t, Pz) : __fsub_rn(t, Pz);
-        // change of M^2 + |P|^2: de (2 t + (1 + |c|^2) de)
-        const float k = (float)(1 + cx * cx + cy * cy + cz * cz);
-        const float s = __fadd_rn(__fmul_rn(2.0f, t), __fmul_rn(k, de));
-        if (__fmul_rn(de, s) < 0.0f) {
+        // the move changes M^2 + |P|^2 by de (2 t + (1 + |c|^2) de), which is
+        // negative exactly when t has the sign of e[q] and |t| exceeds
+        // (1 + |c|^2) / 2 spacings: one for a face, 1.5 for a diagonal
+        const float thr = (cx * cx + cy * cy + cz * cz == 2) ? __fmul_rn(1.5f, ulp) : ulp;
+        if (fabsf(t) > thr && ((__float_as_int(t) ^ __float_as_int(e[q])) >= 0)) {
             d[q] = __fsub_rn(d[q], de);
             M = __fadd_rn(M, de);
             if (cx) Px = cx > 0 ? __fadd_rn(Px, de) : __fsub_rn(Px, de);

@@ -233,7 +233,9 @@ def conserve_round_f16(v):
     counterpart).  v: (n, 19) float32 scaled post-collision values of n cells.
     Every value is rounded to nearest FP16; then for q = 1..18 in order a value
     moves one FP16 spacing towards its exact value when that lowers M^2 + |P|^2
-    (the cell's summed mass and momentum rounding errors so far).  Returns the
+    (the cell's summed mass and momentum rounding errors so far): when the
+    projection t = M + c_q . P has the sign of the value's rounding error and
+    |t| exceeds one spacing (a face direction) or 1.5 (a diagonal).  Returns the
     float32 values of the chosen FP16 numbers.  All arithmetic is float32 with
     one rounding per operation, in the kernel's order."""
     f32 = np.float32
@@ -258,9 +260,11 @@ def conserve_round_f16(v):
         for a in range(3):
             if c[a]:
                 t = (t + P[a] if c[a] > 0 else t - P[a]).astype(f32)
-        k = f32(1 + int((c * c).sum()))
-        s = ((f32(2.0) * t).astype(f32) + (k * de).astype(f32)).astype(f32)
-        move = (de * s).astype(f32) < f32(0.0)
+        # M^2 + |P|^2 falls exactly when t has the sign of e and |t| exceeds
+        # (1 + |c|^2) / 2 spacings
+        thr = (f32(1.5) * ulp).astype(f32) if int((c * c).sum()) == 2 else ulp
+        same_sign = (t.view(np.int32) ^ e[:, q].view(np.int32)) >= 0
+        move = (np.abs(t) > thr) & same_sign
         h[:, q] = np.where(move, (h[:, q] - de).astype(f32), h[:, q])
         M = np.where(move, (M + de).astype(f32), M)
         for a in range(3):
