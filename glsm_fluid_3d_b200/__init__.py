@@ -336,12 +336,18 @@ class Fluid:
         check(self.L.glsm_fluid_profile_velocity(self.h, int(it), _fptr(ms)), "profile_velocity")
         return ms
 
-    def profile_substeps(self, it):
-        """stepVelocity(it) as one captured graph of its substep launches; the
-        time (ms) of the whole graph on the system stream."""
+    def profile_substeps(self, it, n_steps=1):
+        """n_steps calls of stepVelocity(it + j) as one captured graph of their
+        substep launches; the time (ms) of the whole graph on the system stream."""
         out = ctypes.c_float()
-        check(self.L.glsm_fluid_profile_substeps(self.h, int(it), ctypes.byref(out)), "profile_substeps")
+        check(self.L.glsm_fluid_profile_substeps_n(self.h, int(it), int(n_steps), ctypes.byref(out)),
+              "profile_substeps")
         return float(out.value)
+
+    def test_ibm_wait_extra(self, extra):
+        """Test aid: make the force-region tiles wait for `extra` IBM tasks that
+        never run, so the bounded wait gives up (glsm_test_ibm_wait_extra)."""
+        check(self.L.glsm_test_ibm_wait_extra(self.h, int(extra)), "test_ibm_wait_extra")
 
     def conservation(self):
         """(mass, px, py, pz): sum of rho and of c_q f_q over the lattice, reduced

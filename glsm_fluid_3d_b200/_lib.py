@@ -74,6 +74,8 @@ def lib():
         "glsm_fluid_set_deterministic": [vp, i],
         "glsm_gel_filament": [vp, P(d), ctypes.c_size_t, P(ctypes.c_size_t)],
         "glsm_fluid_profile_substeps": [vp, i, P(f)],
+        "glsm_fluid_profile_substeps_n": [vp, i, i, P(f)],
+        "glsm_test_ibm_wait_extra": [vp, i],
         "glsm_gel_set_bz_f": [vp, d],
         "glsm_checkpoint_bytes": [vp, P(ctypes.c_size_t)],
         "glsm_checkpoint_save": [vp, vp, ctypes.c_size_t],

@@ -87,8 +87,9 @@ struct glsm_fluid_s {
     float* scratch = nullptr;    // 19*N floats, allocated on first use
     int lbm_ctas = 0;            // resident CTAs of the persistent substep kernel (odd substeps)
     int lbm_ctas_even = 0;       // the same for even substeps
-    int staged_ctas = 0;         // resident CTAs of the staged substep kernel (0: not used)
-    int l2_on = 0;               // keep the population array L2-persisting (glsm_fluid_set_l2_persisting)
+    int wait_extra = 0;          // test aid (glsm_test_ibm_wait_extra): > 0 makes the IBM wait run out
+    int device = 0;              // CUDA device the system lives on
+    int l2_on = 0;              // keep the population array L2-persisting (glsm_fluid_set_l2_persisting)
     unsigned long long l2_bytes = 0;  // access-policy window of the substep launches (0: none)
     float l2_hit = 0.f;
     double* d_cons = nullptr;    // conservation partial sums (kConsBlocks x 4) and result (4)
@@ -845,19 +846,16 @@ static StepArgs step_args(glsm_fluid f, int k, int iter_arg, bool tail = true) {
     a.div_nx = make_fastdiv((unsigned)f->F.nx);
     a.div_nxy = make_fastdiv((unsigned)(f->F.nx * f->F.ny));
     // full tiles, then half tiles for the last kTailWaves waves of resident
-    // CTAs (none in a batch, whose launches mix systems, nor for the staged
-    // kernel, which stages whole tiles)
+    // CTAs (none in a batch, whose launches mix systems)
     const long long N = f->F.N;
-    const long long tail_cells = (tail && f->staged_ctas == 0)
-                                     ? (long long)kTailWaves * std::max(f->lbm_ctas, 1) * (kTileCells / 2)
-                                     : 0;
+    const long long tail_cells = tail ? (long long)kTailWaves * std::max(f->lbm_ctas, 1) * (kTileCells / 2) : 0;
     const long long big = std::max(0LL, (N - tail_cells) / kTileCells);
     a.big_tiles = (int)big;
     a.n_tiles = (int)(big + (N - big * kTileCells + kTileCells / 2 - 1) / (kTileCells / 2));
     if (tail_cells == 0) a.big_tiles = a.n_tiles = (int)((N + kTileCells - 1) / kTileCells);
     a.lbm_ctas = f->lbm_ctas;
     a.lbm_ctas_even = f->lbm_ctas_even;
-    a.staged_ctas = f->staged_ctas;
+    a.wait_extra = f->wait_extra;
     a.l2_bytes = f->l2_bytes;
     a.l2_hit = f->l2_hit;
     return a;
@@ -870,26 +868,38 @@ static StepArgs step_args(glsm_fluid f, int k, int iter_arg, bool tail = true) {
 // the CUDA context, and L2 it reserves is lost to every access outside a window
 // (a batch's launches, other fluids, the caller's own kernels): it is sized to
 // the largest window of the fluids that use one and released (set to zero,
-// persisting lines reset) when the last of them stops.  Must not run during a
-// capture.
+// persisting lines reset) when the last of them stops.  The set-aside is kept
+// per device: fluids on different devices of one process each size their own.
+// Must not run during a capture.
 static std::mutex g_l2_mu;
-static std::vector<glsm_fluid_s*> g_l2_users;
+static std::vector<glsm_fluid_s*> g_l2_users;  // fluids with a window, on any device
 
-static void l2_setaside_locked() {
+// Sizes device dev's persisting set-aside to the largest window of the fluids
+// on that device (zero, with the persisting lines reset, when none is left) and
+// sets their hit ratios.  Runs with dev current and restores the caller's device.
+static void l2_setaside_locked(int dev) {
+    int prev = dev;
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = dev;
+    if (prev != dev && cudaSetDevice(dev) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
     size_t want = 0;
-    for (auto* u : g_l2_users) want = std::max(want, (size_t)u->l2_bytes);
-    int dev = 0, max_persist = 0;
-    cudaGetDevice(&dev);
+    for (auto* u : g_l2_users)
+        if (u->device == dev) want = std::max(want, (size_t)u->l2_bytes);
+    int max_persist = 0;
     cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev);
     want = std::min(want, (size_t)std::max(max_persist, 0));
     if (cudaDeviceSetLimit(cudaLimitPersistingL2CacheSize, want) != cudaSuccess) cudaGetLastError();
     if (want == 0 && cudaCtxResetPersistingL2Cache() != cudaSuccess) cudaGetLastError();
     size_t cur = 0;
     cudaDeviceGetLimit(&cur, cudaLimitPersistingL2CacheSize);
-    for (auto* u : g_l2_users) u->l2_hit = cur ? std::min(1.0f, (float)cur / (float)u->l2_bytes) : 0.f;
+    for (auto* u : g_l2_users)
+        if (u->device == dev) u->l2_hit = cur ? std::min(1.0f, (float)cur / (float)u->l2_bytes) : 0.f;
+    if (prev != dev) cudaSetDevice(prev);
 }
 
-// enables (on) or disables the window of f and resizes the set-aside
+// enables (on) or disables the window of f and resizes its device's set-aside
 static void l2_window(glsm_fluid f, int on) {
     std::lock_guard<std::mutex> lock(g_l2_mu);
     auto it = std::find(g_l2_users.begin(), g_l2_users.end(), f);
@@ -898,13 +908,13 @@ static void l2_window(glsm_fluid f, int on) {
     f->l2_on = 0;
     f->l2_bytes = 0;
     f->l2_hit = 0.f;
-    int dev = 0, max_window = 0, max_persist = 0;
+    const int dev = f->device;
+    int max_window = 0, max_persist = 0;
     const size_t esz = (f->F.storage == GLSM_STORE_F32) ? 4 : 2;
     const size_t bytes = (size_t)19 * (size_t)f->F.S * esz;
     // only an array that fits in the set-aside can stay resident; a larger
     // one would reserve L2 without the benefit
-    if (on && cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev) == cudaSuccess &&
+    if (on && cudaDeviceGetAttribute(&max_window, cudaDevAttrMaxAccessPolicyWindowSize, dev) == cudaSuccess &&
         cudaDeviceGetAttribute(&max_persist, cudaDevAttrMaxPersistingL2CacheSize, dev) == cudaSuccess &&
         bytes <= (size_t)std::max(max_window, 0) && bytes <= (size_t)std::max(max_persist, 0)) {
         f->l2_on = 1;
@@ -912,12 +922,12 @@ static void l2_window(glsm_fluid f, int on) {
         g_l2_users.push_back(f);
     }
     cudaGetLastError();
-    if (was || f->l2_on) l2_setaside_locked();
+    if (was || f->l2_on) l2_setaside_locked(dev);
     if (f->l2_on && f->l2_hit <= 0.f) {  // no set-aside could be had
         g_l2_users.pop_back();
         f->l2_on = 0;
         f->l2_bytes = 0;
-        l2_setaside_locked();
+        l2_setaside_locked(dev);
     }
 }
 
@@ -957,14 +967,10 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     F.ramp_steps = d->ramp_steps;
     F.nsub = d->nsub;
     const size_t esz = (d->storage == GLSM_STORE_F32) ? 4 : 2;
-    // guard bands before and after the 19 planes: the staged substep kernel
-    // copies whole shifted tile ranges, which for boundary tiles reach up to a
-    // z-plane and a row (plus one tile) beyond the planes
-    const size_t guard = align_up((size_t)d->nx * d->ny + d->nx + 2 * kTileCells + 64, 64);
     size_t bytes;
     {
         Carver cv{nullptr};
-        cv.take<char>((19 * (size_t)F.S + 2 * guard) * esz);
+        cv.take<char>(19 * (size_t)F.S * esz);
         cv.take<float4>(N);
         cv.take<float4>(N);
         for (int i = 0; i < 3; i++) cv.take<float>(N);
@@ -979,7 +985,7 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     }
     f->bytes = bytes;
     Carver cv{(char*)f->arena};
-    F.pop = cv.take<char>((19 * (size_t)F.S + 2 * guard) * esz) + guard * esz;
+    F.pop = cv.take<char>(19 * (size_t)F.S * esz);
     F.u = cv.take<float4>(N);
     F.Fibm = cv.take<float4>(N);
     F.c[0] = cv.take<float>(N);
@@ -1003,15 +1009,7 @@ int glsm_fluid_create(const glsm_fluid_desc* d, glsm_coupler c, glsm_fluid* out)
     fluid_units(d->tau, d->h, c->g2l, c->l2g, nsub_phys);
     f->lbm_ctas = lbm_resident_ctas(d->storage, 1, 0);
     f->lbm_ctas_even = lbm_resident_ctas(d->storage, 0, 0);
-    {
-        static int ctas32 = -1, ctas16 = -1;  // per process (one device type)
-        if (ctas32 < 0) staged_setup(&ctas32, &ctas16);
-        // the shared-memory staged kernel is kept for measurements; the register
-        // kernel is the default
-        const char* kind = getenv("GLSM_LBM_KERNEL");
-        const bool staged = kind && std::strcmp(kind, "staged") == 0;
-        f->staged_ctas = staged ? (d->storage == GLSM_STORE_F32 ? ctas32 : ctas16) : 0;
-    }
+    cudaGetDevice(&f->device);
     f->c = c;
     c->fluid = f;
     // the gels' gather now knows the lattice
@@ -1085,6 +1083,21 @@ int glsm_fluid_set_f16_rounding(glsm_fluid f, int mode) {
     f->F.f16_round = mode;
     f->lbm_ctas = lbm_resident_ctas(f->F.storage, 1, mode);
     f->lbm_ctas_even = lbm_resident_ctas(f->F.storage, 0, mode);
+    // the captured iteration graphs hold the old launch arguments
+    for (auto& row : f->graph)
+        for (auto& g : row)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    return GLSM_OK;
+}
+
+int glsm_test_ibm_wait_extra(glsm_fluid f, int extra) {
+    if (!f || extra < 0) return fail(GLSM_ERR_ARG, "bad argument");
+    if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
+    CK(cudaStreamSynchronize(f->c->stream));
+    f->wait_extra = extra;
     // the captured iteration graphs hold the old launch arguments
     for (auto& row : f->graph)
         for (auto& g : row)
@@ -1219,24 +1232,14 @@ int glsm_fluid_run(glsm_fluid f, int iter0, int n) {
     glsm_coupler c = f->c;
     set_iter_kernel<<<1, 1, 0, c->stream>>>(c->d_ctl, iter0);
     CK(cudaGetLastError());
-    static const bool eager = getenv("GLSM_EAGER") != nullptr;  // debugging: no graphs
     for (int it = 0; it < n; it++) {
         const int p0 = (int)(f->substeps & 1);
-        if (eager) {
-            int r = enqueue_iteration(f, iter0 + it, p0, f->cur);
-            if (r) return r;
-        } else {
-            cudaGraphExec_t ge;
-            int r = get_graph(f, p0, f->cur, &ge);
-            if (r) return r;
-            CK(cudaGraphLaunch(ge, c->stream));
-        }
+        cudaGraphExec_t ge;
+        int r = get_graph(f, p0, f->cur, &ge);
+        if (r) return r;
+        CK(cudaGraphLaunch(ge, c->stream));
         f->substeps += f->F.nsub;
         f->cur ^= 1;
-    }
-    if (eager) {
-        set_iter_kernel<<<1, 1, 0, c->stream>>>(c->d_ctl, iter0 + n);
-        CK(cudaGetLastError());
     }
     return GLSM_OK;
 }
@@ -1281,17 +1284,24 @@ int glsm_fluid_profile_velocity(glsm_fluid f, int iter, float* ms) {
     return r;
 }
 
-// Fluid::stepVelocity as a captured graph of its nsub substep launches, timed
-// with one CUDA event pair around the graph on the system stream: the
-// substep kernel back to back as it runs inside the fused iteration
-int glsm_fluid_profile_substeps(glsm_fluid f, int iter, float* total_ms) {
-    if (!f || !total_ms || iter < 0) return fail(GLSM_ERR_ARG, "bad argument");
+// n_steps calls of Fluid::stepVelocity as one captured graph of their
+// n_steps x nsub substep launches, timed with one CUDA event pair around the
+// graph on the system stream: the substep kernel back to back as it runs inside
+// the fused iteration
+int glsm_fluid_profile_substeps_n(glsm_fluid f, int iter, int n_steps, float* total_ms) {
+    if (!f || !total_ms || iter < 0 || n_steps < 1 || n_steps > 64) return fail(GLSM_ERR_ARG, "bad argument");
     if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
     cudaStream_t s = f->c->stream;
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ge = nullptr;
     CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-    int r = enqueue_velocity(f, iter, s);
+    int r = GLSM_OK;
+    for (int j = 0; j < n_steps && r == GLSM_OK; j++) {
+        // the AA parity of step j follows from the substeps before it
+        r = enqueue_velocity(f, iter + j, s);
+        f->substeps += f->F.nsub;
+    }
+    f->substeps -= (long long)n_steps * f->F.nsub;
     cudaError_t e = cudaStreamEndCapture(s, &g);
     if (r) {
         if (g) cudaGraphDestroy(g);
@@ -1313,8 +1323,12 @@ int glsm_fluid_profile_substeps(glsm_fluid f, int iter, float* total_ms) {
     if (e1) cudaEventDestroy(e1);
     cudaGraphExecDestroy(ge);
     if (e != cudaSuccess) return fail(GLSM_ERR_CUDA, "profile: %s", cudaGetErrorString(e));
-    f->substeps += f->F.nsub;
+    f->substeps += (long long)n_steps * f->F.nsub;
     return GLSM_OK;
+}
+
+int glsm_fluid_profile_substeps(glsm_fluid f, int iter, float* total_ms) {
+    return glsm_fluid_profile_substeps_n(f, iter, 1, total_ms);
 }
 
 static int ensure_scratch(glsm_fluid f) {

@@ -29,7 +29,6 @@ enum : int {
     kErrIbmWait = 1,     // a force-region tile gave up waiting for the IBM tasks
     kErrMarkerOut = 2,   // a marker's 4^3 stencil left the lattice entirely
     kErrNonFinite = 4,   // a non-finite value was met in the gel state
-    kErrStageWait = 8,   // a staged tile's bulk copies did not arrive in time
 };
 
 // inclusive lattice-cell box; empty when x0 > x1

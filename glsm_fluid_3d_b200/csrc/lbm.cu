@@ -313,13 +313,17 @@ __device__ void ibm_task(const StepArgs& a, unsigned task) {
     }
 }
 
-// bounded wait of a force-region tile for the IBM tasks of this substep
+// Bounded wait of a force-region tile for the IBM tasks of this substep.  On
+// time-out the error bit kErrIbmWait is set (the host reports it at the next
+// glsm_fluid_sync) and the tile goes on with the forces spread so far, so the
+// launch always completes and the context stays usable.
 __device__ __forceinline__ void wait_ibm(const StepArgs& a) {
     if (threadIdx.x == 0) {
         const volatile unsigned* flag = a.ibm_done + a.k;
         const volatile int* err = &a.ctl->error;
+        const unsigned target = (unsigned)a.n_ibm + (unsigned)a.wait_extra;
         unsigned spins = 0;
-        while (*flag < (unsigned)a.n_ibm) {
+        while (*flag < target) {
             // give up after ~0.3 s (or at once when another tile already gave up)
             if (++spins > (1u << 22) || (*err & kErrIbmWait)) {
                 atomicOr(&a.ctl->error, kErrIbmWait);
@@ -530,8 +534,7 @@ __device__ __forceinline__ void store_u(const StepArgs& a, unsigned i, bool inb,
     if (inb || a.last) a.F.u[i] = u;
 }
 
-// force, collision and AA-pattern scatter of one cell (shared by the register
-// and the shared-memory staged gathers)
+// force, collision and AA-pattern scatter of one cell
 template <int ST, int PARITY, int PERX>
 __device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, unsigned x, bool fast, bool xin,
                                                 bool inb, float (&d)[19]) {
@@ -881,270 +884,6 @@ __global__ void __launch_bounds__(kTile, (lbm_ctas_per_sm<ST, PARITY>())) lbm_su
     }
 }
 
-
-// ---------------------------------------------------------------------------
-// staged substep: each tile's 19 population ranges are brought into shared
-// memory by one-dimensional bulk copies (TMA) one tile ahead of the compute
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
-__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-        : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// order this thread's (and, after a barrier, the CTA's) generic-proxy accesses
-// to shared memory before the following async-proxy (bulk copy) writes
-__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
-        "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-
-template <int ST>
-struct Stage {
-    using T = typename PopIO<ST>::T;
-    static constexpr int PAD = 16 / (int)sizeof(T);      // one 16-byte vector of elements
-    static constexpr int PLANE = kTileCells + PAD;       // staged elements per direction
-    static constexpr unsigned BYTES = PLANE * sizeof(T); // bytes per direction (a multiple of 16)
-    static constexpr size_t BUF = 19 * (size_t)BYTES;    // one staged tile
-    static constexpr int CTAS = (ST == kStoreF32) ? 2 : 3;
-};
-
-// thread 0: bulk copies of the 19 ranges tile `tile` reads.  For direction q the
-// range starts at the tile's first cell (even substeps, slot q) or at the first
-// cell's upstream neighbour x - c_q (odd substeps, slot opp q), rounded down to
-// 16 bytes; shift[q] is the rounding.  Ranges of boundary tiles may reach into
-// the guard bands around the population array; the lanes that would use such
-// values (walls, wraps) read global memory instead.
-template <int ST, int PARITY>
-__device__ __forceinline__ void issue_tile_loads(const StepArgs& a, unsigned tile, typename Stage<ST>::T* buf,
-                                                 int* shift, unsigned long long* bar) {
-    using T = typename Stage<ST>::T;
-    constexpr int PAD = Stage<ST>::PAD;
-    const FluidDev& F = a.F;
-    const long long S = F.S, nx = F.nx, nxy = (long long)F.nx * F.ny;
-    const long long c0 = (long long)tile * kTileCells;
-    const T* P = reinterpret_cast<const T*>(F.pop);
-    fence_proxy_async_smem();
-    mbar_arrive_expect_tx(bar, 19u * Stage<ST>::BYTES);
-#pragma unroll
-    for (int q = 0; q < 19; q++) {
-        const long long off = qcx(q) + qcy(q) * nx + qcz(q) * nxy;
-        const long long start = PARITY == 0 ? (long long)q * S + c0 : (long long)qopp(q) * S + c0 - off;
-        const long long al = start & ~(long long)(PAD - 1);
-        shift[q] = (int)(start - al);
-        bulk_copy_g2s(buf + q * Stage<ST>::PLANE, P + al, Stage<ST>::BYTES, bar);
-    }
-}
-
-// gather of one cell from the staged tile (li: the cell's index in the tile)
-template <int ST, int PARITY, int PERX>
-__device__ __forceinline__ void lbm_cell_staged(const StepArgs& a, unsigned i, unsigned li, bool inb,
-                                                const typename Stage<ST>::T* sb, const int* shift) {
-    using IO = PopIO<ST>;
-    using T = typename IO::T;
-    constexpr int PL = Stage<ST>::PLANE;
-    const FluidDev& F = a.F;
-    const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
-    const unsigned S = (unsigned)F.S, nxy = nx * ny;
-    const unsigned z = fdiv(i, a.div_nxy);
-    const unsigned rem = i - z * nxy;
-    const unsigned y = fdiv(rem, a.div_nx);
-    const unsigned x = rem - y * nx;
-    const T* P = reinterpret_cast<const T*>(F.pop);
-    float d[19];
-    bool fast = true;
-    if (PARITY == 1) fast = __all_sync(__activemask(), (y - 1u < ny - 2u) && (z - 1u < nz - 2u));
-    if (PARITY == 0) {
-#pragma unroll
-        for (int q = 0; q < 19; q++) d[q] = IO::raw(sb + q * PL + li);
-    } else if (fast) {
-#pragma unroll
-        for (int q = 0; q < 19; q++) {
-            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
-            const T* sq = sb + q * PL + li + shift[q];
-            if (cx == 0) {
-                d[q] = IO::raw(sq);
-            } else {
-                // x walls (bounce: own slot q) or x wraps (periodic x) read global memory
-                const bool edge = (cx > 0) ? (x == 0) : (x == nx - 1);
-                if (edge) {
-                    const unsigned nbr = i - (unsigned)(cx + cy * (int)nx + cz * (int)nxy);
-                    d[q] = IO::raw(P + (PERX ? qopp(q) * S + nbr + (unsigned)(cx * (int)nx) : q * S + i));
-                } else {
-                    d[q] = IO::raw(sq);
-                }
-            }
-        }
-    } else {
-        int mo[3], po[3];
-        bool mw[3], pw[3], mr[3], pr[3];
-        const unsigned c[3] = {x, y, z}, n[3] = {nx, ny, nz}, st[3] = {1u, nx, nxy};
-#pragma unroll
-        for (int k = 0; k < 3; k++) {
-            mw[k] = pw[k] = mr[k] = pr[k] = false;
-            mo[k] = -(int)st[k];
-            po[k] = (int)st[k];
-            if (c[k] == 0) {
-                if (F.per[k]) {
-                    mo[k] = (int)((n[k] - 1) * st[k]);
-                    mr[k] = true;
-                } else {
-                    mw[k] = true;
-                }
-            }
-            if (c[k] == n[k] - 1) {
-                if (F.per[k]) {
-                    po[k] = -(int)((n[k] - 1) * st[k]);
-                    pr[k] = true;
-                } else {
-                    pw[k] = true;
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 19; q++) {
-            const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
-            const bool wall = (cx > 0 && mw[0]) || (cx < 0 && pw[0]) || (cy > 0 && mw[1]) || (cy < 0 && pw[1]) ||
-                              (cz > 0 && mw[2]) || (cz < 0 && pw[2]);
-            const bool wrap = (cx > 0 && mr[0]) || (cx < 0 && pr[0]) || (cy > 0 && mr[1]) || (cy < 0 && pr[1]) ||
-                              (cz > 0 && mr[2]) || (cz < 0 && pr[2]);
-            if (wall) {
-                d[q] = IO::raw(P + (q * S + i));
-            } else if (wrap) {
-                const int off = (cx > 0 ? mo[0] : cx < 0 ? po[0] : 0) + (cy > 0 ? mo[1] : cy < 0 ? po[1] : 0) +
-                                (cz > 0 ? mo[2] : cz < 0 ? po[2] : 0);
-                d[q] = IO::raw(P + (qopp(q) * S + i + (unsigned)off));
-            } else {
-                d[q] = IO::raw(sb + q * PL + li + shift[q]);
-            }
-        }
-    }
-    collide_scatter<ST, PARITY, PERX>(a, i, x, fast, false, inb, d);
-}
-
-// bounded wait for a staged tile; on time-out the error flag is set and the
-// (invalid) tile is computed anyway, so that no copy is left in flight
-__device__ __forceinline__ void wait_stage(const StepArgs& a, unsigned long long* bar, unsigned parity) {
-    unsigned spins = 0;
-    while (!mbar_try_wait(bar, parity)) {
-        if (++spins > (1u << 22)) {
-            atomicOr(&a.ctl->error, kErrStageWait);
-            break;
-        }
-    }
-}
-
-template <int ST, int PARITY, int PERX>
-__global__ void __launch_bounds__(kTile, Stage<ST>::CTAS) lbm_substep_staged_kernel(StepArgs a) {
-    using T = typename Stage<ST>::T;
-    extern __shared__ __align__(128) unsigned char dsmem[];
-    // staged tile buffers 0 and 1
-    auto buf = [&](int b) { return reinterpret_cast<T*>(dsmem + (b ? Stage<ST>::BUF : 0)); };
-    __shared__ TileSlot s_slot[2];
-    __shared__ int s_shift[2][19];
-    __shared__ __align__(8) unsigned long long s_bar[2];
-    const unsigned total = (unsigned)a.n_ibm + (unsigned)a.n_tiles;
-    const unsigned n_ibm = (unsigned)a.n_ibm;
-    const bool warp0 = threadIdx.x < 32;
-    unsigned next = 0;  // thread 0: the ticket after the prepared one
-    if (threadIdx.x == 0) {
-        mbar_init(&s_bar[0], 1);
-        mbar_init(&s_bar[1], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    if (warp0) {
-        unsigned t0 = 0;
-        if (threadIdx.x == 0) {
-            t0 = atomicAdd(&a.tickets[a.k], 1u);
-            next = atomicAdd(&a.tickets[a.k], 1u);
-            if (t0 >= n_ibm && t0 < total) issue_tile_loads<ST, PARITY>(a, t0 - n_ibm, buf(0), s_shift[0], &s_bar[0]);
-        }
-        t0 = __shfl_sync(0xffffffffu, t0, 0);
-        prepare_slot(a, t0, s_slot[0]);
-    }
-    __syncthreads();
-    unsigned phase = 0;  // bit j: the parity of s_bar[j]'s current phase
-    for (int j = 0;; j ^= 1) {
-        const unsigned t = s_slot[j].t;
-        if (t >= total) break;
-        if (warp0) {
-            unsigned tn = 0;
-            if (threadIdx.x == 0) {
-                tn = next;
-                next = atomicAdd(&a.tickets[a.k], 1u);
-                // the other buffer was last read before the previous barrier
-                if (tn >= n_ibm && tn < total)
-                    issue_tile_loads<ST, PARITY>(a, tn - n_ibm, buf(j ^ 1), s_shift[j ^ 1], &s_bar[j ^ 1]);
-            }
-            tn = __shfl_sync(0xffffffffu, tn, 0);
-            prepare_slot(a, tn, s_slot[j ^ 1]);
-        }
-        if (t < n_ibm) {
-            ibm_task(a, t);
-        } else {
-            const TileSlot& sl = s_slot[j];
-            const int nb = sl.nb;
-            if (nb > 0) wait_ibm(a);
-            wait_stage(a, &s_bar[j], (phase >> j) & 1u);
-            phase ^= 1u << j;
-            const FluidDev& F = a.F;
-            const unsigned c0 = (t - n_ibm) * kTileCells;
-            const unsigned c1 = min(c0 + kTileCells - 1, (unsigned)F.N - 1);
-#pragma unroll 1
-            for (int r = 0; r < kCellsPerThread; r++) {
-                const unsigned li = r * kTile + threadIdx.x;
-                const unsigned i = c0 + li;
-                if (i <= c1) {
-                    const bool inb = nb > 0 && (F.det_spread ? in_boxes<true>(a, sl, nb, i) : in_boxes<false>(a, sl, nb, i));
-                    lbm_cell_staged<ST, PARITY, PERX>(a, i, li, inb, buf(j), s_shift[j]);
-                }
-            }
-        }
-        __syncthreads();
-    }
-}
-
-template <int ST, int PARITY, int PERX>
-static int staged_ctas_and_attr() {
-    auto k = lbm_substep_staged_kernel<ST, PARITY, PERX>;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * Stage<ST>::BUF));
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kTile, 2 * Stage<ST>::BUF);
-    return max(1, sms * max(1, per_sm));
-}
-
-// dynamic shared memory attributes of every staged instance; returns the
-// resident CTAs of the FP32 and the 16-bit kernels
-void staged_setup(int* ctas32, int* ctas16) {
-    *ctas32 = staged_ctas_and_attr<kStoreF32, 0, 0>();
-    staged_ctas_and_attr<kStoreF32, 1, 0>();
-    staged_ctas_and_attr<kStoreF32, 1, 1>();
-    *ctas16 = staged_ctas_and_attr<kStoreF16, 0, 0>();
-    staged_ctas_and_attr<kStoreF16, 1, 0>();
-    staged_ctas_and_attr<kStoreF16, 1, 1>();
-    staged_ctas_and_attr<kStoreBF16, 0, 0>();
-    staged_ctas_and_attr<kStoreBF16, 1, 0>();
-    staged_ctas_and_attr<kStoreBF16, 1, 1>();
-}
 
 // ---------------------------------------------------------------------------
 // batched substep: several systems in one persistent launch
@@ -1539,25 +1278,6 @@ int lbm_resident_ctas(int storage, int parity, int f16_round) {
 }
 
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
-    if (a.staged_ctas > 0 && a.F.f16_round == 0) {
-        const int total = a.n_ibm + a.n_tiles;
-        const dim3 g(min(total, a.staged_ctas)), b(kTile);
-#define GLSM_STAGED(ST)                                                                          \
-    if (parity && a.F.per[0])                                                                    \
-        lbm_substep_staged_kernel<ST, 1, 1><<<g, b, 2 * Stage<ST>::BUF, s>>>(a);                 \
-    else if (parity)                                                                             \
-        lbm_substep_staged_kernel<ST, 1, 0><<<g, b, 2 * Stage<ST>::BUF, s>>>(a);                 \
-    else                                                                                         \
-        lbm_substep_staged_kernel<ST, 0, 0><<<g, b, 2 * Stage<ST>::BUF, s>>>(a);
-        switch (a.F.storage) {
-            case kStoreF32: GLSM_STAGED(kStoreF32); break;
-            case kStoreF16: GLSM_STAGED(kStoreF16); break;
-            case kStoreBF16: GLSM_STAGED(kStoreBF16); break;
-            default: return cudaErrorInvalidValue;
-        }
-#undef GLSM_STAGED
-        return cudaGetLastError();
-    }
     dim3 grid(lbm_grid(a, parity)), block(kTile);
     // substeps after the first are launched with programmatic stream
     // serialization (the kernel waits for its predecessor itself,

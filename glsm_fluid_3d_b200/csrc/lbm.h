@@ -21,7 +21,8 @@ struct StepArgs {
     int big_tiles;       // tiles [0, big_tiles) hold kTileCells cells, the rest kTileCells / 2
     int lbm_ctas;        // persistent CTAs per odd-substep launch (0: one per ticket)
     int lbm_ctas_even;   // persistent CTAs per even-substep launch (0: one per ticket)
-    int staged_ctas;     // > 0: the shared-memory staged kernel with this many CTAs
+    int wait_extra;      // test aid: IBM tasks a force-region tile waits for beyond n_ibm (> 0 makes the
+                         // bounded wait run out; 0 in every normal launch)
     float l2_hit;        // > 0: substep launches mark the first l2_bytes of the population
     unsigned long long l2_bytes;  // array L2-persisting with this hit ratio
 };
@@ -70,7 +71,6 @@ cudaError_t launch_conv_diff_batch(const BatchSys* sys, const int* block_offsets
 cudaError_t launch_batch_advance(const BatchSys* sys, int n, cudaStream_t s);
 int batch_resident_ctas(const BatchGroupKey& g, int parity);
 int lbm_resident_ctas(int storage, int parity, int f16_round);
-void staged_setup(int* ctas32, int* ctas16);
 cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s);
 cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s);
 cudaError_t launch_read_pop(const FluidDev& F, int natural, float* out, cudaStream_t s);

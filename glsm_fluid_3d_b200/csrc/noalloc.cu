@@ -15,6 +15,14 @@
 // call; every GPU that loads the library holds the 5,308,416-byte array until
 // the process exits.  All calls on a device share the array: calls that
 // overlap on the GPU (different streams without ordering) race on it.
+//
+// Set-up: the first call on a device (with that device current) looks up the
+// array's device address with cudaGetSymbolAddress and caches it together with
+// the device's current context; a later call on a new context of that device
+// (after cudaDeviceReset, or a primary context released and re-created, where
+// the module and its array are loaded anew) repeats the look-up.  Make the
+// first call on a device before any stream capture.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
@@ -79,8 +87,13 @@ __global__ void na_stencil(unsigned char* scratch, const float4* lag, int M, flo
     const int l = blockIdx.x * blockDim.x + threadIdx.x;
     if (l >= M) return;
     const float4 p = lag[l];
-    const float g[3] = {p.x / h, p.y / h, p.z / h};
     const int n[3] = {nx, ny, nz};
+    // a non-finite or far-out position gives a fully clipped stencil (the
+    // marker then neither samples nor spreads); within 8 cells of the lattice
+    // the position is used as it is (a stencil reaches 2 cells)
+    const bool fin = isfinite(p.x) && isfinite(p.y) && isfinite(p.z);
+    float g[3] = {p.x / h, p.y / h, p.z / h};
+    for (int d = 0; d < 3; d++) g[d] = fin ? fminf(fmaxf(g[d], -8.f), (float)n[d] + 8.f) : -8.f;
     int b0[3], valid = 0;
     float ph[3][4];
     for (int d = 0; d < 3; d++) {
@@ -223,7 +236,24 @@ __global__ void na_lbm(const unsigned char* scratch, float* pop, unsigned S, flo
 thread_local char g_na_err[256] = "";
 std::mutex g_na_mutex;
 constexpr int kNaMaxDevices = 64;
-void* g_na_ptr[kNaMaxDevices] = {};
+void* g_na_ptr[kNaMaxDevices] = {};       // the scratch's device address per device
+CUcontext g_na_ctx[kNaMaxDevices] = {};   // the context that address belongs to
+
+// cuCtxGetCurrent through the runtime's driver entry point (no link against
+// the driver library); null when the driver does not provide it
+using CtxGetCurrent = CUresult (*)(CUcontext*);
+CtxGetCurrent ctx_get_current() {
+    static const CtxGetCurrent fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        cudaGetLastError();
+        return reinterpret_cast<CtxGetCurrent>(p);
+    }();
+    return fn;
+}
 
 int na_fail(int code, const char* msg) {
     snprintf(g_na_err, sizeof(g_na_err), "%s", msg);
@@ -259,14 +289,19 @@ int glsm_substep_noalloc(float* pop, int64_t plane_stride, float* u4, int nx, in
         return na_fail(GLSM_ERR_CUDA, "no current CUDA device");
     unsigned char* scratch = nullptr;
     {
-        // set-up, once per device, with that device current: the device
-        // address of the scratch array (the first call on a device does this)
+        // set-up, once per device and context, with that device current: the
+        // device address of the scratch array (the first call on a device does
+        // this, and the first call after the device's context was re-created)
         std::lock_guard<std::mutex> lock(g_na_mutex);
-        if (!g_na_ptr[dev]) {
+        CUcontext ctx = nullptr;
+        const CtxGetCurrent get_ctx = ctx_get_current();
+        const bool known_ctx = get_ctx && get_ctx(&ctx) == CUDA_SUCCESS && ctx;
+        if (!g_na_ptr[dev] || !known_ctx || ctx != g_na_ctx[dev]) {
             void* p = nullptr;
             const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
             if (e != cudaSuccess || !p) return na_fail(GLSM_ERR_CUDA, "cudaGetSymbolAddress of the scratch failed");
             g_na_ptr[dev] = p;
+            g_na_ctx[dev] = known_ctx ? ctx : nullptr;
         }
         scratch = static_cast<unsigned char*>(g_na_ptr[dev]);
     }

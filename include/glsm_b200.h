@@ -287,6 +287,19 @@ int glsm_fluid_profile_velocity(glsm_fluid f, int iter, float* ms);
  * with a single CUDA event pair around it: *total_ms is the time of the nsub
  * launches back to back, as they run inside the fused iteration graph. */
 int glsm_fluid_profile_substeps(glsm_fluid f, int iter, float* total_ms);
+/* n_steps (1..64) calls of Fluid::stepVelocity(iter + j) as one captured graph
+ * of n_steps x nsub substep launches with one CUDA event pair around it.  The
+ * difference between two n_steps values, divided by the substeps between them,
+ * is the substep launch time without the graph's launch overhead (one 2 x nsub
+ * word ticket reset per velocity step is included). */
+int glsm_fluid_profile_substeps_n(glsm_fluid f, int iter, int n_steps, float* total_ms);
+/* Test aid for the bounded device waits (no counterpart in the reference):
+ * extra > 0 makes every force-region tile of the following substep launches
+ * wait for `extra` IBM tasks that do not exist, so the wait gives up after its
+ * limit (a fraction of a second), the launch completes with the forces spread
+ * so far, and the next glsm_fluid_sync reports GLSM_ERR_DEVICE with
+ * "IBM wait timed out".  extra = 0 (the default) restores normal launches. */
+int glsm_test_ibm_wait_extra(glsm_fluid f, int extra);
 /* gel_to_lbm_vel and lbm_to_gel_vel (src/fluid.cu:221-222) */
 int glsm_fluid_units(glsm_fluid f, float out[2]);
 

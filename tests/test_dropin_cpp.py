@@ -10,7 +10,19 @@ import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
-REF_SIM = "/root/reference/src/sim.cpp"  # present only where the reference is mounted
+
+
+def _reference_sim():
+    """The reference's src/sim.cpp where the reference is mounted: GLSM_REF_SRC,
+    else the directory the oracle build recorded in oracle/_ref/ref_src."""
+    d = os.environ.get("GLSM_REF_SRC")
+    rec = os.path.join(ROOT, "oracle", "_ref", "ref_src")
+    if not d and os.path.exists(rec):
+        d = open(rec).read().strip()
+    return os.path.join(d, "sim.cpp") if d else ""
+
+
+REF_SIM = _reference_sim()
 
 
 def compile_driver(src, exe):
