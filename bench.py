@@ -88,6 +88,11 @@ def parse():
     p.add_argument("--no-l2-persisting", action="store_true",
                    help="leave the population array's L2 access-policy window off")
     p.add_argument("--cpu-seconds", type=float, default=12.0, help="budget of the CPU baseline sample")
+    p.add_argument("--no-f16", action="store_true", help="skip the FP16 forms' sub-object")
+    p.add_argument("--f16-steps", type=int, default=300, help="timed steps of each FP16 form")
+    p.add_argument("--no-serving", action="store_true", help="skip the serving sub-object")
+    p.add_argument("--serving-requests", type=int, default=64)
+    p.add_argument("--serving-step-scale", type=float, default=0.1)
     return p.parse_args()
 
 
@@ -255,6 +260,97 @@ def cpu_baseline(budget_s):
                       f"(oracle/glsm_oracle.cpp, OpenMP), {dt:.1f} s"}
 
 
+def barrier(world):
+    """All ranks here and the device idle."""
+    import torch
+
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+
+
+def timed_steps(s, K, warmup, world, it0=0):
+    """K coupled iterations of system s, each between CUDA events on the system
+    stream, with the persisting L2 lines released and L2 flushed before each;
+    returns (total device ms over the K steps, next iteration, clock stats)."""
+    import torch
+
+    from glsm_fluid_3d_b200 import l2_reset_persisting
+
+    fluid = s.fluid
+    stream = torch.cuda.ExternalStream(s.coupler.stream())
+    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    it = it0
+    for _ in range(warmup):
+        fluid.run(it, 1)
+        it += 1
+    fluid.sync()
+    clocks = Clocks(torch.cuda.current_device())
+    clocks.start()
+    time.sleep(0.3)  # let the sampler settle
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    barrier(world)
+    t_wall0 = time.time()
+    for k in range(K):
+        # between timed steps: the previous step done, its persisting L2 lines
+        # (the population array's access-policy window) released, L2 flushed
+        stream.synchronize()
+        l2_reset_persisting()
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[k][0].record(stream)
+            fluid.run(it, 1)
+            ev[k][1].record(stream)
+        it += 1
+    stream.synchronize()
+    barrier(world)
+    clk = clocks.stop(t_wall0, time.time())
+    fluid.sync()
+    return sum(a.elapsed_time(b) for a, b in ev), it, clk
+
+
+def substep_roofline(s, storage, it, l2):
+    """Achieved bandwidth of the substep kernel: graphs of one and of two velocity
+    steps (nsub and 2 nsub substep launches) timed with one event pair each on
+    the system stream; their difference over nsub is the launch time without
+    the graph's launch overhead.  Returns (roofline dict, next iteration)."""
+    import statistics as st
+
+    fluid = s.fluid
+    one, two, prof = [], [], []
+    for rep in range(9):
+        if rep < 6:
+            n = 1 + rep % 2
+            t = fluid.profile_substeps(it, n_steps=n)
+            (one if n == 1 else two).append(t)
+        else:
+            n = 1
+            prof.extend(fluid.profile_velocity(it).tolist())
+        for j in range(n):  # keep the state consistent for what follows
+            s.coupler.packFromGels()
+            fluid.stepConcentration(it + j)
+        it += n
+    fluid.sync()
+    avg_ms = (st.median(two) - st.median(one)) / NSUB
+    N = DIMS[0] * DIMS[1] * DIMS[2]
+    bpc = BYTES_PER_CELL[storage]
+    achieved = bpc * N / (avg_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+            "frac": round(achieved / peak, 4), "traffic": ncu_traffic(storage), "peak_kind": peak_kind,
+            "l2_peak": round(l2, 1), "frac_l2": round(achieved / l2, 4),
+            "l2_peak_how": f"glsm_copy_bandwidth: 2 x {L2_PROBE_BYTES >> 20} MiB copied back and forth "
+                           f"{L2_PROBE_REPS} times in one launch, L1 bypassed (measured in this run)",
+            "kernel": "lbm_substep_kernel", "bytes_per_launch": bpc * N, "avg_launch_ms": round(avg_ms, 5),
+            "avg_launch_ms_one_graph": round(st.median(one) / NSUB, 5),
+            "avg_launch_ms_event_pairs": round(st.mean(prof), 5),
+            "timing": f"graphs of {NSUB} and {2 * NSUB} substep launches (one and two velocity steps), 3 each, "
+                      f"one event pair around each graph: (median 2-step - median 1-step) / {NSUB}",
+            "note": "algorithmic bytes = one read + one write of 19 populations per cell; the 78 MB population "
+                    "array of 101^3 fits in L2, so achieved can exceed the HBM copy peak"}
+    return roof, it
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -276,78 +372,15 @@ def run_ours(args, world, rank, local):
     s = make_system(args.storage)
     fluid = s.fluid
     fluid.set_l2_persisting(not args.no_l2_persisting)  # one system alone on the GPU
-    stream = torch.cuda.ExternalStream(s.coupler.stream())
-    flush = torch.empty(FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
-    clocks = Clocks(local)
-    clocks.start()
-    it = 0
-    for _ in range(args.warmup):
-        fluid.run(it, 1)
-        it += 1
-    fluid.sync()
-    time.sleep(0.3)  # let the sampler settle
-
-    def barrier():
-        if world > 1:
-            torch.distributed.barrier()
-        torch.cuda.synchronize()
-
     K = args.steps
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-    barrier()
-    t_wall0 = time.time()
-    from glsm_fluid_3d_b200 import l2_reset_persisting
-
-    for k in range(K):
-        # between timed steps: the previous step done, its persisting L2 lines
-        # (the population array's access-policy window) released, L2 flushed
-        stream.synchronize()
-        l2_reset_persisting()
-        with torch.cuda.stream(stream):
-            flush.zero_()
-            ev[k][0].record(stream)
-            fluid.run(it, 1)
-            ev[k][1].record(stream)
-        it += 1
-    stream.synchronize()
-    barrier()
-    t_wall1 = time.time()
-    clk = clocks.stop(t_wall0, t_wall1)
-    fluid.sync()
-    t_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in ev), world, "cuda")
+    t_ms, it, clk = timed_steps(s, K, args.warmup, world)
+    t_ms = max_over_ranks(t_ms, world, "cuda")
     N = DIMS[0] * DIMS[1] * DIMS[2]
     value = job_value(N, NSUB, K, world, t_ms / 1e3)
 
-    # dominant kernel: the substep kernel.  Each velocity step's nsub launches
-    # run as one captured graph timed by an event pair on the system stream
-    # (as inside the fused iteration); per-launch event pairs, which add the
-    # launch latency to every launch, are reported beside it
-    graph_ms, prof = [], []
-    for rep in range(6):
-        if rep < 3:
-            graph_ms.append(fluid.profile_substeps(it) / NSUB)
-        else:
-            prof.extend(fluid.profile_velocity(it).tolist())
-        s.coupler.packFromGels()  # keep the state consistent for what follows
-        fluid.stepConcentration(it)
-        it += 1
-    fluid.sync()
-    avg_ms = statistics.mean(graph_ms)
-    bpc = BYTES_PER_CELL[args.storage]
-    achieved = bpc * N / (avg_ms / 1e3) / 1e9
-    peak, peak_kind = peaks()
-    traffic = ncu_traffic(args.storage)
-    roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-            "frac": round(achieved / peak, 4), "traffic": traffic, "peak_kind": peak_kind,
-            "l2_peak": round(l2, 1), "frac_l2": round(achieved / l2, 4),
-            "l2_peak_how": f"glsm_copy_bandwidth: 2 x {L2_PROBE_BYTES >> 20} MiB copied back and forth "
-                           f"{L2_PROBE_REPS} times in one launch, L1 bypassed (measured in this run)",
-            "kernel": "lbm_substep_kernel", "bytes_per_launch": bpc * N, "avg_launch_ms": round(avg_ms, 5),
-            "avg_launch_ms_event_pairs": round(statistics.mean(prof), 5),
-            "timing": "3 velocity steps, each a captured graph of its substep launches between one event pair, "
-                      "divided by the launches",
-            "note": "algorithmic bytes = one read + one write of 19 populations per cell; the 78 MB population "
-                    "array of 101^3 fits in L2, so achieved can exceed the HBM copy peak"}
+    # dominant kernel: the substep kernel, timed as it runs inside the fused
+    # iteration (graphs of its launches on the system stream)
+    roof, it = substep_roofline(s, args.storage, it, l2)
 
     # end to end through the C ABI with host buffers: restart the state from
     # pinned host memory, run K iterations reading the gels' node velocities back
@@ -371,7 +404,7 @@ def run_ours(args, world, rank, local):
         h2d = sum(a.nbytes + b.nbytes + c.nbytes for a, b, c in zip(host_rn, host_um, host_vm)) + host_u.nbytes + \
             host_c.nbytes
         d2h = K * sum(v.nbytes for v in host_vel) + host_u.nbytes + host_c.nbytes
-        barrier()
+        barrier(world)
         t0 = time.perf_counter()
         for g, a, b, c in zip(gels, host_rn, host_um, host_vm):
             g.write("rn", a)
@@ -386,7 +419,7 @@ def run_ours(args, world, rank, local):
                 g.read_into("Veln", v)
         fluid.read_into("u", host_u)
         fluid.read_into("c1", host_c)
-        barrier()
+        barrier(world)
         t_e2e = max_over_ranks(time.perf_counter() - t0, world, "cuda")
         e2e = {"value": round(job_value(N, NSUB, K, world, t_e2e), 1), "unit": "MLUPS",
                "h2d_bytes_per_step": int(h2d / K), "d2h_bytes_per_step": int(d2h / K),
@@ -396,9 +429,16 @@ def run_ours(args, world, rank, local):
                       "and c read back (D2H); bytes are totals divided by K"}
         assert np.isfinite(host_u).all()
 
+    s.close()
     base = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         base = cpu_baseline(args.cpu_seconds)
+    f16 = None
+    if world == 1 and args.storage == "f32" and not args.no_f16:
+        f16 = f16_forms(args, value, l2)
+    serve = None
+    if world == 1 and args.workload == "D" and not args.no_serving:
+        serve = serving_summary(args)
 
     launches_per_step = 1 + 1 + 1 + 1 + NSUB + 1  # set-iter, gel, concentration markers, repulsion, substeps, conv-diff
     line = {
@@ -409,12 +449,58 @@ def run_ours(args, world, rank, local):
         "roofline": roof, "cpu_baseline": base, "e2e": e2e,
         "clocks": clk, "gpu_launches": launches_per_step * K,
     }
-    s.close()
+    if f16 is not None:
+        line["f16"] = f16
+    if serve is not None:
+        line["serving"] = serve
     if world > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def f16_forms(args, f32_value, l2):
+    """The FP16-storage forms on the same workload and timing method, with fewer
+    timed steps: nearest rounding and the conserving rounding (the form that
+    keeps the 10,000-iteration velocity error within 1e-3)."""
+    out = {}
+    N = DIMS[0] * DIMS[1] * DIMS[2]
+    K = max(1, min(args.steps, args.f16_steps))
+    for storage in ("f16", "f16c"):
+        s = make_system(storage)
+        s.fluid.set_l2_persisting(not args.no_l2_persisting)
+        t_ms, it, clk = timed_steps(s, K, args.warmup, 1)
+        roof, it = substep_roofline(s, storage, it, l2)
+        s.close()
+        v = job_value(N, NSUB, K, 1, t_ms / 1e3)
+        out[storage] = {"value": round(v, 1), "unit": "MLUPS", "steps": K, "ms_per_step": round(t_ms / K, 4),
+                        "vs_f32": round(v / f32_value, 3),
+                        "roofline": {k: roof[k] for k in ("achieved", "peak", "unit", "frac", "l2_peak", "frac_l2",
+                                                          "bytes_per_launch", "avg_launch_ms", "traffic")},
+                        "clocks": clk}
+    out["note"] = ("FP16 deviations f_q - w_q scaled by 2^20, FP32 collision; f16 rounds to nearest, f16c with the "
+                   "mass- and momentum-conserving rounding; same workload, L2 flush and timing as the headline")
+    return out
+
+
+def serving_summary(args):
+    """A short run of the serving ensemble (continuous batching with HBM-budget
+    admission) beside the same requests run one after another with the plain
+    FP32 form: aggregate MLUPS, p50/p99 completion latency, speed-up."""
+    from glsm_fluid_3d_b200 import serving
+
+    reqs = serving.make_requests(args.serving_requests, 8.0, 2024, args.serving_step_scale)
+    stats = serving.Server(150e9).serve(reqs).summary()
+    base, _ = serving.sequential(reqs)
+    return {"aggregate_mlups": stats["aggregate_mlups"], "p50_latency_s": stats["p50_latency_s"],
+            "p99_latency_s": stats["p99_latency_s"], "makespan_s": stats["makespan_s"],
+            "sequential_plain_f32_mlups": base["mlups"], "sequential_s": base["seconds"],
+            "speedup_vs_sequential": round(stats["aggregate_mlups"] / base["mlups"], 3),
+            "requests": len(reqs), "max_resident_systems": stats["max_resident_systems"],
+            "config": {"arrivals": "seeded Poisson, 8 per second", "sides": list(serving.SIDES),
+                       "gels": "1-4 of 4-8 elements", "steps": f"500-5000 x {args.serving_step_scale}",
+                       "storage": "FP32 / FP16 half and half", "budget_gb": 150}}
 
 
 def run_reference(args, world, rank, local):

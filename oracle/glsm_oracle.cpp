@@ -229,6 +229,40 @@ struct Gel {
                         bIndex[count++] = i + j * (LX + 2) + k * (LX + 2) * (LY + 2);
     }
 
+    // Gel::buildTubeMask, gel.cu:811-867: tube axis along x at the element
+    // centre, inner half-extents = half the node extent minus the wall; void
+    // elements (the tube's lumen) restart at the steady state.  Float
+    // arithmetic as in the reference.
+    void build_tube_mask(int wall, bool circular) {
+        float cy = (LY + 1) * 0.5f, cz = (LZ + 1) * 0.5f;
+        float ihy = (LY * 0.5f) - wall, ihz = (LZ * 0.5f) - wall;
+        if (ihy <= 0) ihy = 0;
+        if (ihz <= 0) ihz = 0;
+        tube_mode = circular ? 2 : 1;
+        tube_cy = cy;
+        tube_cz = cz;
+        tube_ihy = ihy;
+        tube_ihz = ihz;
+        for (int zi = 1; zi <= LZ; zi++)
+            for (int yi = 1; yi <= LY; yi++) {
+                float dyv = (float)yi - cy, dzv = (float)zi - cz;
+                bool v;
+                if (circular) {
+                    float r2 = dyv * dyv / (ihy * ihy + 1e-6f) + dzv * dzv / (ihz * ihz + 1e-6f);
+                    v = (ihy > 0 && ihz > 0 && r2 < 1.0f);
+                } else {
+                    v = (std::fabs(dyv) < ihy && std::fabs(dzv) < ihz);
+                }
+                if (!v) continue;
+                for (int xi = 1; xi <= LX; xi++) {
+                    int gi = E(xi, yi, zi);
+                    um[gi] = uss;
+                    vm[gi] = vss;
+                    wm[gi] = wss;
+                }
+            }
+    }
+
     void add_noise(uint64_t seed, double amp) {
         for (int zi = 1; zi < LZ; zi++)
             for (int yi = 1; yi < LY; yi++)
@@ -1211,6 +1245,8 @@ int orc_gel_control(void* p, int gel, int what, double value) {
                 G.anchor_z = value;
                 break;
             case 3: G.active_from = (int)value; break;
+            case 4: G.build_tube_mask((int)value, false); break;  // square tube, wall = value
+            case 5: G.build_tube_mask((int)value, true); break;   // cylindrical tube
             default: return -1;
         }
     });

@@ -119,6 +119,9 @@ class Oracle:
     def set_active_from(self, gel, it):
         assert self.L.orc_gel_control(self.h, gel, 3, float(it)) == 0
 
+    def build_tube_mask(self, gel, wall_thickness, circular=False):
+        assert self.L.orc_gel_control(self.h, gel, 5 if circular else 4, float(wall_thickness)) == 0
+
     def finalize(self):
         assert self.L.orc_finalize(self.h) == 0
 

@@ -44,6 +44,9 @@ def lib():
         L.ref_field.argtypes = [vp, i, i, ctypes.POINTER(d), ll]
         L.ref_destroy.argtypes = [vp]
         L.ref_last_error.restype = ctypes.c_char_p
+        L.ref_record_center.argtypes = [vp, i]
+        L.ref_write_files.argtypes = [vp, i]
+        L.ref_set_start_time.argtypes = [vp, i]
         _lib = L
     return _lib
 
@@ -66,6 +69,11 @@ class Reference:
         if self.h:
             self.L.ref_destroy(self.h)
             self.h = None
+
+    def set_start_time(self, t):
+        """Gels added afterwards and the fluid restart from the .dat files of
+        time t in the current directory (the reference's setGoonValue)."""
+        self._chk(self.L.ref_set_start_time(self.h, int(t)), "start time")
 
     def set_params(self, beta=1.0, ramp_steps=20000.0):
         # Fluid::stepVelocity reads IBM_RAMP_STEPS on every call (src/fluid.cu:265-268)
@@ -94,6 +102,19 @@ class Reference:
 
     def set_active_from(self, gel, it):
         self._chk(self.L.ref_gel_control(self.h, gel, 3, float(it)), "active")
+
+    def build_tube_mask(self, gel, wall_thickness, circular=False):
+        self._chk(self.L.ref_gel_control(self.h, gel, 5 if circular else 4, float(wall_thickness)), "tube")
+
+    def record_center(self, iter):
+        """Gel::recordCenter(iter) of every gel (src/gel.cu:706-712)."""
+        self._chk(self.L.ref_record_center(self.h, iter), "recordCenter")
+
+    def write_files(self, iter):
+        """Gel::writeFiles(iter) of every gel and Fluid::writeFiles(iter)
+        (src/gel.cu:543-553, src/fluid.cu:140-150) into the current directory;
+        the writer threads are joined before this returns."""
+        self._chk(self.L.ref_write_files(self.h, iter), "writeFiles")
 
     def finalize(self):
         self._chk(self.L.ref_finalize(self.h), "finalize")

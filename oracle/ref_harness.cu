@@ -40,6 +40,7 @@ namespace {
 
 struct RefSim {
     int nx, ny, nz, nsub;
+    int start_time = 0;  // > 0: gels and fluid restart from the .dat files of that time (setGoonValue)
     std::vector<Gel*> gels;
     std::vector<int> active_from;
     Coupler* coupler = nullptr;
@@ -105,7 +106,7 @@ void* ref_create(int nx, int ny, int nz, int nsub) {
 int ref_add_gel(void* p, int sx, int sy, int sz, double px, double py, double pz, int type, int id) {
     auto* s = (RefSim*)p;
     if (s->fluid) return -1;
-    Gel* g = new Gel(make_int3(sx, sy, sz), make_double3(px, py, pz), type, id, 0);
+    Gel* g = new Gel(make_int3(sx, sy, sz), make_double3(px, py, pz), type, id, s->start_time);
     int LX = g->m_gelNodeGrid.x, LY = g->m_gelNodeGrid.y;
     if (pad_map(g->m_dmap_node, g->m_hmap_node, g->m_numGelNodes, g->m_gridDim2, LX + 2, LY + 2)) return -1;
     if (pad_map(g->m_dmap_element, g->m_hmap_element, g->m_numGelElements, g->m_gridDim1, LX + 1, LY + 1))
@@ -130,6 +131,11 @@ int ref_add_gel(void* p, int sx, int sy, int sz, double px, double py, double pz
     zero(g->m_dFdrag_robin, nN);
     zero(g->m_dVeln, nN);
     zero(g->m_dVels, nN);
+    zero(g->m_dvm_center, 1000);
+    zero(g->m_dwm_center, 1000);
+    zero(g->m_drm_center, 1000);
+    zero(g->m_dFn_center, 1000);
+    zero(g->m_dVeln_center, 1000);
     if (check(cudaDeviceSynchronize(), "add_gel")) return -1;
     s->gels.push_back(g);
     s->active_from.push_back(0);
@@ -163,9 +169,19 @@ int ref_gel_control(void* p, int gi, int what, double value) {
         case 1: g->fireExcitationPulse(); break;
         case 2: g->setAnchorZ(value); break;
         case 3: s->active_from[gi] = (int)value; break;
+        case 4: g->buildTubeMask((int)value, false); break;
+        case 5: g->buildTubeMask((int)value, true); break;
         default: return -1;
     }
     return check(cudaDeviceSynchronize(), "control");
+}
+
+// gels added after this call and the fluid restart from the .dat files of
+// time t in the current directory (the constructors' setGoonValue,
+// src/gel.cu:221-282, src/fluid.cu:57-83)
+int ref_set_start_time(void* p, int t) {
+    ((RefSim*)p)->start_time = t;
+    return 0;
 }
 
 int ref_set_beta(void* p, double beta) {
@@ -180,7 +196,7 @@ int ref_finalize(void* p) {
     s->coupler = new Coupler(s->gels);
     // smallest odd lattice >= the requested one: 2*fs + 1 cells per axis
     int3 fs = make_int3((s->nx) / 2, (s->ny) / 2, (s->nz) / 2);
-    s->fluid = new Fluid(fs, 0, s->coupler);
+    s->fluid = new Fluid(fs, s->start_time, s->coupler);
     Fluid* F = s->fluid;
     F->h_fp->beta = s->beta;
     if (F->fluidNodeGrid.x != s->nx || F->fluidNodeGrid.y != s->ny || F->fluidNodeGrid.z != s->nz) {
@@ -257,6 +273,39 @@ double ref_time(void* p, int iter0, int n) {
     return ms;
 }
 
+// Gel::recordCenter(iter) of every gel.  Its calFilamentD stores up to
+// maxFilamentlen crossings per record without a bound check
+// (src/gel_kernels.cu:837-866), so only gels with at most that many node faces
+// (every crossing lies on its own face) are accepted.
+int ref_record_center(void* p, int iter) {
+    auto* s = (RefSim*)p;
+    for (auto* g : s->gels) {
+        const long long faces = (long long)(g->m_gelNodeGrid.x - 1) * (g->m_gelNodeGrid.y - 1) *
+                                (g->m_gelNodeGrid.z - 1);
+        if (faces > g->m_hgp->maxFilamentlen) {
+            snprintf(g_err, sizeof(g_err), "recordCenter: gel with %lld node faces exceeds the filament buffer", faces);
+            return -1;
+        }
+    }
+    for (auto* g : s->gels) g->recordCenter(iter);
+    return check(cudaDeviceSynchronize(), "recordCenter");
+}
+
+// Gel::writeFiles(iter) of every gel and Fluid::writeFiles(iter), written into
+// the current directory; the writer threads are joined before returning (the
+// reference joins them at the next write or in its destructors)
+int ref_write_files(void* p, int iter) {
+    auto* s = (RefSim*)p;
+    if (!s->fluid) return -1;
+    if (check(cudaDeviceSynchronize(), "writeFiles pre")) return -1;
+    for (auto* g : s->gels) g->writeFiles(iter);
+    s->fluid->writeFiles(iter);
+    for (auto* g : s->gels)
+        if (g->m_file_writer_thread.joinable()) g->m_file_writer_thread.join();
+    if (s->fluid->file_writer_thread.joinable()) s->fluid->file_writer_thread.join();
+    return check(cudaDeviceSynchronize(), "writeFiles");
+}
+
 int ref_info(void* p, long long* out) {
     auto* s = (RefSim*)p;
     out[0] = s->fluid ? s->fluid->N : 0;
@@ -318,6 +367,12 @@ long long ref_field(void* p, int field, int gi, double* buf, long long n) {
             case 38: src = g->m_dvm_norm; count = nE; break;
             case 39: src = g->m_dwmp; count = nE; break;
             case 40: src = g->m_dFn_robin; count = 3 * nN; break;
+            // the centre-element records of recordCenter, slot (iter / 1000) % 1000
+            case 41: src = g->m_dvm_center; count = 1000; break;
+            case 42: src = g->m_dwm_center; count = 1000; break;
+            case 43: src = g->m_drm_center; count = 3 * 1000; break;
+            case 44: src = g->m_dFn_center; count = 3 * 1000; break;
+            case 45: src = g->m_dVeln_center; count = 3 * 1000; break;
             default: return -1;
         }
     }

@@ -27,3 +27,17 @@ def gpu():
     if not have_gpu():
         pytest.fail("this test needs a CUDA GPU")
     return True
+
+
+@pytest.fixture(autouse=True)
+def _ibm_env():
+    """The reference reads IBM_BETA / IBM_RAMP_STEPS from the environment on
+    every velocity step (src/fluid.cu:199, :266) and oracle/pyref.py sets them;
+    restore both after each test so that no test sees another's settings."""
+    saved = {k: os.environ.get(k) for k in ("IBM_BETA", "IBM_RAMP_STEPS")}
+    yield
+    for k, v in saved.items():
+        if v is None:
+            os.environ.pop(k, None)
+        else:
+            os.environ[k] = v

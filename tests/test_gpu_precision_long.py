@@ -1,12 +1,17 @@
-"""Long-horizon accuracy of FP16 population storage: the absolute bound of the
-precision form, 1e-3 relative L2 in the lattice velocity and in the gel
-displacement rn - rn(0), after 10,000 coupled iterations.
+"""Long-horizon accuracy of FP16 population storage: the bound of the precision
+form, 1e-3 relative L2 in the lattice velocity and in the gel displacement
+rn - rn(0), after 10,000 coupled iterations.
 
-Workload: the small configuration (48^3 lattice, one centred 6x6x6-element gel,
-Nsub = 2, IBM ramp 20,000, seeded chemistry noise).  The FP32 solver stands in
-for the FP64 oracle here: on this workload it stays within ~2e-6 (u) and ~1e-14
-(gel fields) of the oracle (test_gpu_workloads.py), three orders of magnitude
-inside the bound, and the oracle itself would need hours for 10,000 iterations.
+Workloads: the default one (101^3 lattice, two 6x6x6-element gels, Nsub = 25:
+250,000 substeps) and the small one (48^3, one centred gel, Nsub = 2), both
+with the IBM ramp 20,000 and seeded chemistry noise.  The FP32 solver stands
+in for the FP64 oracle: on the default workload it stays within 5.5e-6 (u) and
+~1e-14 (gel fields) of the oracle after 10,000 iterations, far inside the
+bound, and the oracle itself would need hours for 10,000 iterations.
+
+Round-to-nearest FP16 accumulates long-wavelength noise over many substeps
+(1.3e-3 at 101^3); the conserving rounding ("f16c") keeps the error near one
+rounding's worth and is the form held to the bound there.
 """
 import numpy as np
 import pytest
@@ -20,8 +25,8 @@ ITERS = 10_000
 BOUND = 1e-3
 
 
-def _run(storage):
-    bench.select("S")
+def _run(workload, storage):
+    bench.select(workload)
     try:
         s = bench.make_system(storage)
         n = len(bench.W["gels"])
@@ -34,14 +39,16 @@ def _run(storage):
         bench.select("D")
 
 
-def test_f16_storage_within_bound_after_10k_iterations(gpu):
-    ref = _run("f32")
+@pytest.mark.parametrize("workload,held", [("D", ("f16c",)), ("S", ("f16", "f16c2", "f16c"))])
+def test_f16_storage_within_bound_after_10k_iterations(gpu, workload, held):
+    ref = _run(workload, "f32")
     errs = {}
     for storage in ("f16", "f16c2", "f16c"):
-        got = _run(storage)
+        got = _run(workload, storage)
         errs[storage] = {k: rel_l2(got[k], ref[k]) for k in ref}
-        print(f"S/{ITERS} {storage:6s} u rel_l2={errs[storage]['u']:.2e} disp rel_l2={errs[storage]['disp']:.2e}")
-    # the conserving form meets both bounds; every form meets the displacement bound
-    assert errs["f16c"]["u"] <= BOUND, errs
-    for storage, e in errs.items():
+        print(f"{workload}/{ITERS} {storage:6s} u rel_l2={errs[storage]['u']:.2e} "
+              f"disp rel_l2={errs[storage]['disp']:.2e}")
+    for storage in held:
+        assert errs[storage]["u"] <= BOUND, (storage, errs)
+    for storage, e in errs.items():  # every form meets the displacement bound
         assert e["disp"] <= BOUND, (storage, e)

@@ -14,9 +14,15 @@ every lattice, marker and gel field after the same number of iterations.
   iterations.
 
 Tolerances are relative L2 norms.  The reference stores absolute FP32
-populations f (round-off ~6e-8 of f ~ w_q), the product FP32 deviations
-f - w_q, so the two differ by the reference's own FP32 round-off; the FP64
-oracle is computed beside them to show where that floor lies.
+populations f (round-off ~3e-8 of f ~ w_q), the product FP32 deviations
+f - w_q, so the two differ by the reference's own FP32 round-off.  The FP64
+oracle is run beside them and sets that floor: a field passes when the product
+is within TOL_ORACLE of the oracle, and within TOL_REF of the reference or no
+farther from the reference than the exact (FP64) answer is.  Under the IBM ramp
+of the benchmark (beta_eff = beta (iter + 1) / 20,000) the first iterations'
+velocity is of the order of the reference's round-off, so there the floor
+decides; a second run with the ramp off (full penalty from the first step)
+compares a velocity field three orders of magnitude larger.
 """
 import numpy as np
 import pytest
@@ -33,6 +39,12 @@ DEFAULT = dict(dims=(101, 101, 101), nsub=25, beta=1.0, ramp=20000.0, seed=12345
 SMALL = dict(dims=(48, 48, 48), nsub=2, beta=1.0, ramp=20000.0, seed=12345, amp=1e-3, save_pop=False,
              gels=[dict(size=(6, 6, 6), pos=(11.75, 11.75, 11.75), type=1)])
 
+# product vs the FP64 oracle (as in test_gpu_parity.py)
+TOL_ORACLE = {
+    "u": 2e-4, "Ul": 2e-4, "Fdrag": 2e-5, "pop": 1e-6, "rho": 1e-6, "c1": 1e-5, "Dl": 1e-5,
+    "Sl": 1e-5, "Cl": 1e-5, "Frep": 1e-5, "lag": 1e-7, "Vl": 1e-6, "un_robin": 1e-5, "un_norm": 1e-6,
+}
+GEL_TOL_ORACLE = 1e-8
 # product vs the reference build (both FP32 on the fluid side, FP64 gels)
 TOL_REF = {
     "u": 2e-3, "Ul": 1e-3, "Fdrag": 1e-4, "pop": 1e-5, "rho": 1e-5, "c1": 1e-5, "Dl": 1e-5,
@@ -54,56 +66,60 @@ def _run(cls, case, iters, **kw):
     return out
 
 
-def _compare(got, want, label, tol=TOL_REF, gel_tol=GEL_TOL_REF, floor=None):
+def _tol(k, tol, gel_tol):
+    name = k.split("_", 1)[1] if k.startswith("g") and "_" in k else k
+    return tol.get(name, gel_tol if k.startswith("g") else 1e-4)
+
+
+def _compare(got, ref, orc, label):
+    """Per field: product vs oracle within TOL_ORACLE, and product vs reference
+    within TOL_REF or within 1.05x (plus 1e-12) of oracle vs reference."""
     bad, rows = [], []
-    for k in want:
+    for k in ref:
         if k.endswith("_T1"):
             continue  # round-off sized on both sides (faces that close the element)
-        name = k.split("_", 1)[1] if k.startswith("g") and "_" in k else k
-        t = tol.get(name, gel_tol if k.startswith("g") else 1e-4)
-        e = rel_l2(got[k], want[k])
-        f = f" (oracle vs reference {floor[k]:.2e})" if floor is not None and k in floor else ""
-        rows.append(f"{label} {k:14s} rel_l2={e:.2e} tol={t:.0e}{f}")
-        if not e <= t:
-            bad.append((k, e, t))
+        t_ref, t_orc = _tol(k, TOL_REF, GEL_TOL_REF), _tol(k, TOL_ORACLE, GEL_TOL_ORACLE)
+        e_ref, e_orc, floor = rel_l2(got[k], ref[k]), rel_l2(got[k], orc[k]), rel_l2(orc[k], ref[k])
+        amax = float(np.abs(np.asarray(ref[k])).max()) if np.size(ref[k]) else 0.0
+        rows.append(f"{label} {k:14s} vs-ref={e_ref:.2e} (tol {t_ref:.0e}, oracle-vs-ref {floor:.2e}) "
+                    f"vs-oracle={e_orc:.2e} (tol {t_orc:.0e}) max|ref|={amax:.2e}")
+        if not (e_orc <= t_orc and (e_ref <= t_ref or e_ref <= 1.05 * floor + 1e-12)):
+            bad.append((k, e_ref, e_orc, floor))
     print("\n".join(rows))
     return bad
 
 
-def test_default_workload_vs_reference_build(gpu):
-    """101^3, two gels, Nsub = 25, 20 iterations: the benchmark's workload."""
+def _three(case, iters, methods=False):
     from glsm_fluid_3d_b200 import System
 
     _need_reference()
-    iters = 20
-    ref = _run(pyref.Reference, DEFAULT, iters)
-    got = _run(System, DEFAULT, iters)
-    orc = _run(pyoracle.Oracle, DEFAULT, iters)
-    floor = {k: rel_l2(orc[k], ref[k]) for k in ref}
-    bad = _compare(got, ref, "D/20 product-vs-reference", floor=floor)
+    ref = _run(pyref.Reference, case, iters)
+    got = _run(System, case, iters, methods=methods)
+    orc = _run(pyoracle.Oracle, case, iters)
+    return got, ref, orc
+
+
+def test_default_workload_vs_reference_build(gpu):
+    """101^3, two gels, Nsub = 25, IBM ramp 20,000, 20 iterations: the
+    benchmark's workload through the fused graph path."""
+    bad = _compare(*_three(DEFAULT, 20), "D/20")
+    assert not bad, bad
+
+
+def test_default_workload_full_penalty_vs_reference_build(gpu):
+    """The same lattice and gels with the IBM ramp off, 20 iterations."""
+    bad = _compare(*_three(dict(DEFAULT, ramp=0.0), 20), "D-ramp0/20")
     assert not bad, bad
 
 
 def test_default_workload_methods_path_vs_reference_build(gpu):
-    """The same workload through the per-method calls of the drop-in API (the
-    reference driver's loop, src/sim.cpp:97-112), 10 iterations."""
-    from glsm_fluid_3d_b200 import System
-
-    _need_reference()
-    iters = 10
-    ref = _run(pyref.Reference, DEFAULT, iters)
-    got = _run(System, DEFAULT, iters, methods=True)
-    bad = _compare(got, ref, "D/10 methods-vs-reference")
+    """The default workload through the per-method calls of the drop-in API (the
+    reference driver's loop, src/sim.cpp:97-112), ramp off, 10 iterations."""
+    bad = _compare(*_three(dict(DEFAULT, ramp=0.0), 10, methods=True), "D-ramp0/10 methods")
     assert not bad, bad
 
 
 def test_small_workload_1000_iterations_vs_reference_build(gpu):
     """48^3, one gel, Nsub = 2, 1,000 iterations against the reference build."""
-    from glsm_fluid_3d_b200 import System
-
-    _need_reference()
-    iters = 1000
-    ref = _run(pyref.Reference, SMALL, iters)
-    got = _run(System, SMALL, iters)
-    bad = _compare(got, ref, "S/1000 product-vs-reference")
+    bad = _compare(*_three(SMALL, 1000), "S/1000")
     assert not bad, bad
