@@ -235,8 +235,10 @@ def test_tube_mask_vs_reference_and_oracle(gpu, circular):
     bad = []
     for k in ("u", "c1", "g0_um", "g0_vm", "g0_wm", "g0_rn", "g0_Veln", "g0_un_norm"):
         e_orc, e_ref, floor = rel_l2(got[k], orc[k]), rel_l2(got[k], ref[k]), rel_l2(orc[k], ref[k])
-        t_orc = 2e-4 if k in ("u",) else (1e-5 if k in ("c1",) else 1e-8)
-        t_ref = 2e-3 if k in ("u",) else (1e-5 if k in ("c1",) else 1e-6)
+        # u, c1 and un_norm (which carries the FP32 Robin flux) as in
+        # test_gpu_parity.py; the FP64 gel fields to 1e-8 of the oracle
+        t_orc = {"u": 2e-4, "c1": 1e-5, "g0_un_norm": 1e-6}.get(k, 1e-8)
+        t_ref = {"u": 2e-3, "c1": 1e-5, "g0_un_norm": 1e-5}.get(k, 1e-6)
         print(f"tube {'cyl' if circular else 'sq'} {k:12s} vs oracle {e_orc:.2e}  vs reference {e_ref:.2e} "
               f"(oracle vs reference {floor:.2e})")
         if not (e_orc <= t_orc and (e_ref <= t_ref or e_ref <= 1.05 * floor + 1e-12)):

@@ -39,10 +39,15 @@ DEFAULT = dict(dims=(101, 101, 101), nsub=25, beta=1.0, ramp=20000.0, seed=12345
 SMALL = dict(dims=(48, 48, 48), nsub=2, beta=1.0, ramp=20000.0, seed=12345, amp=1e-3, save_pop=False,
              gels=[dict(size=(6, 6, 6), pos=(11.75, 11.75, 11.75), type=1)])
 
-# product vs the FP64 oracle (as in test_gpu_parity.py)
+# product vs the FP64 oracle (as in test_gpu_parity.py).  The marker
+# concentration Cl, the Robin flux Sl and its nodal sum un_robin are FP32 in the
+# product and the reference and FP64 in the oracle; in the first iterations they
+# are small (max |Cl| 1e-4 after 10 iterations), so their FP32 round-off is
+# 1e-5 to 3e-5 of their norm -- the product and the reference then agree with
+# each other to 5e-6 and both differ from the oracle by that amount.
 TOL_ORACLE = {
     "u": 2e-4, "Ul": 2e-4, "Fdrag": 2e-5, "pop": 1e-6, "rho": 1e-6, "c1": 1e-5, "Dl": 1e-5,
-    "Sl": 1e-5, "Cl": 1e-5, "Frep": 1e-5, "lag": 1e-7, "Vl": 1e-6, "un_robin": 1e-5, "un_norm": 1e-6,
+    "Sl": 5e-5, "Cl": 5e-5, "Frep": 1e-5, "lag": 1e-7, "Vl": 1e-6, "un_robin": 5e-5, "un_norm": 1e-6,
 }
 GEL_TOL_ORACLE = 1e-8
 # product vs the reference build (both FP32 on the fluid side, FP64 gels)
