@@ -784,150 +784,6 @@ __device__ __forceinline__ void lbm_pair_even(const StepArgs& a, unsigned i0, bo
     for (int q = 0; q < 19; q++) Pv[qopp(q) * LS2] = r[q];
 }
 
-// 32-bit view of a pair vector (half2 / bfloat162) for warp shuffles
-template <typename V>
-__device__ __forceinline__ V shfl_up1(V v) {
-    unsigned u = *reinterpret_cast<unsigned*>(&v);
-    u = __shfl_up_sync(0xffffffffu, u, 1);
-    return *reinterpret_cast<V*>(&u);
-}
-template <typename V>
-__device__ __forceinline__ V shfl_down1(V v) {
-    unsigned u = *reinterpret_cast<unsigned*>(&v);
-    u = __shfl_down_sync(0xffffffffu, u, 1);
-    return *reinterpret_cast<V*>(&u);
-}
-
-// Odd substep of two adjacent cells i0 (even) and i0 + 1 of 16-bit storage,
-// one thread per pair, lanes holding consecutive pairs.  The pair's 19 arriving
-// populations come from slots opp(q) at i0 - off_q and i0 + 1 - off_q and its
-// post-collision values go to slots q at i0 + off_q and i0 + 1 + off_q
-// (off_q = c_q . (1, nx, nx ny)).  For an even off_q both are one aligned
-// 4-byte vector; for an odd off_q they straddle two vectors, of which the lane
-// loads (stores) one and passes the other half to (from) its neighbour lane
-// with a shuffle; lanes 0 and 31 cover the warp's two outer halves with single
-// 2-byte accesses.  A warp takes this path only when its 64 cells all lie in
-// the tile and off the y and z boundary planes; in a warp that holds x-wall
-// cells the directions with c_x != 0 go one cell at a time with the wall (or
-// periodic wrap) chosen per lane, as in lbm_cell.  Each slot a lane reads for a
-// neighbour was read (not yet written) by this warp, and each slot a vector
-// store writes belongs to one of the warp's cells, so the in-place update of the
-// AA pattern is unchanged.  Other warps take lbm_cell for each cell.
-template <int ST, int PERX>
-__device__ __forceinline__ void lbm_pair_odd(const StepArgs& a, unsigned i0, unsigned c1, bool inb0, bool inb1) {
-    using IO = PopIO<ST>;
-    using T = typename IO::T;
-    using PIO = PairIO<ST>;
-    using V = typename PIO::V;
-    const FluidDev& F = a.F;
-    const unsigned nx = F.nx, ny = F.ny, nz = F.nz, nxy = nx * ny;
-    const unsigned S = (unsigned)F.S;
-    const unsigned lane = threadIdx.x & 31;
-    const unsigned z0 = fdiv(i0, a.div_nxy);
-    const unsigned r0 = i0 - z0 * nxy;
-    const unsigned y0 = fdiv(r0, a.div_nx);
-    const unsigned x0 = r0 - y0 * nx;
-    // the pair's second cell: next in x, or the first of the next row / plane
-    unsigned x1 = x0 + 1, y1 = y0, z1 = z0;
-    if (x1 == nx) {
-        x1 = 0;
-        if (++y1 == ny) {
-            y1 = 0;
-            z1++;
-        }
-    }
-    const bool yz0 = (y0 - 1u < ny - 2u) && (z0 - 1u < nz - 2u);
-    const bool yz1 = (y1 - 1u < ny - 2u) && (z1 - 1u < nz - 2u);
-    const bool fast = __all_sync(0xffffffffu, i0 + 1 <= c1 && yz0 && yz1);
-    if (!fast) {
-        if (i0 <= c1) lbm_cell<ST, 1, PERX>(a, i0, inb0);
-        if (i0 + 1 <= c1) lbm_cell<ST, 1, PERX>(a, i0 + 1, inb1);
-        return;
-    }
-    const bool xin = __all_sync(0xffffffffu, (x0 - 1u < nx - 2u) && (x1 - 1u < nx - 2u));
-    T* P = reinterpret_cast<T*>(F.pop);
-    V v[19];
-#pragma unroll
-    for (int q = 0; q < 19; q++) {
-        const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
-        const int off = cx + cy * (int)nx + cz * (int)nxy;
-        const T* src = P + (size_t)qopp(q) * S + i0;  // slot opp(q) of cell i0; minus off_q: the upstream cell
-        if (cx != 0 && !xin) {
-            // one cell at a time: across an x wall the bounced opp(q) population
-            // of the cell itself (slot q), or the wrapped neighbour (periodic x)
-            const bool e0 = (cx > 0) ? (x0 == 0) : (x0 == nx - 1);
-            const bool e1 = (cx > 0) ? (x1 == 0) : (x1 == nx - 1);
-            T lo, hi;
-            if (PERX) {
-                lo = src[e0 ? cx * (int)nx - off : -off];
-                hi = src[1 + (e1 ? cx * (int)nx - off : -off)];
-            } else {
-                lo = e0 ? P[(size_t)q * S + i0] : src[-off];
-                hi = e1 ? P[(size_t)q * S + i0 + 1] : src[1 - off];
-            }
-            v[q] = PIO::make(lo, hi);
-        } else if ((off & 1) == 0) {
-            v[q] = *reinterpret_cast<const V*>(src - off);
-        } else {
-            const V w = *reinterpret_cast<const V*>(src - off + 1);  // (i0 + 1 - off, i0 + 2 - off)
-            V prev = shfl_up1(w);                                    // the lane below: (i0 - 1 - off, i0 - off)
-            if (lane == 0) prev = *reinterpret_cast<const V*>(src - off - 1);
-            v[q] = PIO::make(PIO::hi_raw(prev), PIO::lo_raw(w));
-        }
-    }
-    {
-        float d[19];
-#pragma unroll
-        for (int q = 0; q < 19; q++) d[q] = PIO::lo(v[q]);
-        store_u(a, i0, inb0, force_collide<ST>(a, i0, inb0, d));
-        if constexpr (IO::kConserve) conserve_round(d);
-#pragma unroll
-        for (int q = 0; q < 19; q++) v[q] = PIO::set_lo(v[q], d[q]);
-    }
-    {
-        float d[19];
-#pragma unroll
-        for (int q = 0; q < 19; q++) d[q] = PIO::hi(v[q]);
-        store_u(a, i0 + 1, inb1, force_collide<ST>(a, i0 + 1, inb1, d));
-        if constexpr (IO::kConserve) conserve_round(d);
-#pragma unroll
-        for (int q = 0; q < 19; q++) v[q] = PIO::set_hi(v[q], d[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < 19; q++) {
-        const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
-        const int off = cx + cy * (int)nx + cz * (int)nxy;
-        T* dst = P + (size_t)q * S + i0;  // slot q of cell i0; plus off_q: the downstream cell
-        if (cx != 0 && !xin) {
-            // one cell at a time: beyond an x wall the value bounces back into
-            // slot opp(q) of the cell itself, or wraps (periodic x)
-            const bool e0 = (cx > 0) ? (x0 == nx - 1) : (x0 == 0);
-            const bool e1 = (cx > 0) ? (x1 == nx - 1) : (x1 == 0);
-            if (PERX) {
-                dst[e0 ? off - cx * (int)nx : off] = PIO::lo_raw(v[q]);
-                dst[1 + (e1 ? off - cx * (int)nx : off)] = PIO::hi_raw(v[q]);
-            } else {
-                if (e0) P[(size_t)qopp(q) * S + i0] = PIO::lo_raw(v[q]);
-                else dst[off] = PIO::lo_raw(v[q]);
-                if (e1) P[(size_t)qopp(q) * S + i0 + 1] = PIO::hi_raw(v[q]);
-                else dst[1 + off] = PIO::hi_raw(v[q]);
-            }
-        } else if ((off & 1) == 0) {
-            *reinterpret_cast<V*>(dst + off) = v[q];
-        } else {
-            // i0 + off is odd: the pair's values are the high half of the vector
-            // at i0 + off - 1 and the low half of the one at i0 + off + 1, whose
-            // high half is the next lane's first value
-            const V nxt = shfl_down1(v[q]);
-            if (lane < 31)
-                *reinterpret_cast<V*>(dst + off + 1) = PIO::make(PIO::hi_raw(v[q]), PIO::lo_raw(nxt));
-            else
-                dst[off + 1] = PIO::hi_raw(v[q]);
-            if (lane == 0) dst[off] = PIO::lo_raw(v[q]);
-        }
-    }
-}
-
 // whether cell i lies in a marker box of the tile; with deterministic spreads a
 // box cell also gathers its IBM force from the markers of the boxes that hold
 // it (gel order, then marker order) into Fibm[i], where the collision reads it
@@ -953,20 +809,18 @@ __device__ __forceinline__ bool in_boxes(const StepArgs& a, const TileSlot& sl, 
 }
 
 // a lattice tile of consecutive cells (tile_range), up to kCellsPerThread per
-// thread: adjacent pairs with FP16 storage, else cells kTile apart
+// thread: adjacent pairs on even substeps of FP16 storage, else cells kTile apart
 template <int ST, int PARITY, int PERX, bool PAIR = false, bool DET = false>
 __device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const TileSlot& sl) {
     unsigned c0, c1;
     tile_range(a, tile, c0, c1);
     const int nb = sl.nb;
     if (nb > 0) wait_ibm(a);
-    if constexpr (PAIR && (ST == kStoreF16 || ST == kStoreF16C) && kCellsPerThread == 2) {
+    if constexpr (PAIR && PARITY == 0 && (ST == kStoreF16 || ST == kStoreF16C) && kCellsPerThread == 2) {
         const unsigned i0 = c0 + 2 * threadIdx.x;
         const bool inb0 = nb > 0 && i0 <= c1 && in_boxes<DET>(a, sl, nb, i0);
         const bool inb1 = nb > 0 && i0 + 1 <= c1 && in_boxes<DET>(a, sl, nb, i0 + 1);
-        if constexpr (PARITY == 1) {
-            lbm_pair_odd<ST, PERX>(a, i0, c1, inb0, inb1);  // every lane of the warp takes part
-        } else if (i0 + 1 <= c1) {
+        if (i0 + 1 <= c1) {
             lbm_pair_even<ST>(a, i0, inb0, inb1);
         } else if (i0 <= c1) {
             lbm_cell<ST, PARITY, PERX>(a, i0, inb0);
@@ -990,8 +844,8 @@ __device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const
 template <int ST, int PARITY>
 constexpr int lbm_ctas_per_sm() {
     // 64 registers (4 CTAs of 256 threads per SM); 80 (3 CTAs) for the paired
-    // substeps of FP16 storage, whose threads hold two cells
-    return (ST == kStoreF16 || ST == kStoreF16C) ? 768 / kTile : 1024 / kTile;
+    // even substeps of FP16 storage, whose threads hold two cells
+    return (PARITY == 0 && (ST == kStoreF16 || ST == kStoreF16C)) ? 768 / kTile : 1024 / kTile;
 }
 
 template <int ST, int PARITY, int PERX, bool DET>
@@ -1115,11 +969,11 @@ __device__ void prepare_batch_slot(const BatchLaunch& L, unsigned t, BatchSlot& 
 // The batched tiles read the system's parameters from the shared-memory slot
 // rather than from the constant bank; on even substeps that costs registers
 // (at 64 a thread spills about 170 bytes), so the batched even substeps take
-// 80 registers (3 CTAs of 256 threads per SM) and the odd ones, one cell per
-// thread, 64.
+// 80 registers (3 CTAs of 256 threads per SM) and the odd ones the
+// single-system budget.
 template <int ST, int PARITY>
 constexpr int batch_ctas_per_sm() {
-    return PARITY == 0 ? 768 / kTile : 1024 / kTile;
+    return PARITY == 0 ? 768 / kTile : lbm_ctas_per_sm<ST, PARITY>();
 }
 
 // Tickets: first the group's IBM tasks, then its tiles, so the
@@ -1151,9 +1005,7 @@ __global__ void __launch_bounds__(kTile, (batch_ctas_per_sm<ST, PARITY>())) lbm_
         } else if (sl.is_ibm) {
             ibm_task(sl.a, sl.local);
         } else {
-            // the paired FP16 path on even substeps only: the paired odd path
-            // needs more registers than the batch's odd budget leaves
-            lbm_tile<ST, PARITY, PERX, PARITY == 0, DET>(sl.a, sl.local, sl.ts);
+            lbm_tile<ST, PARITY, PERX, true, DET>(sl.a, sl.local, sl.ts);
         }
         if (warp0) {
             tn = __shfl_sync(0xffffffffu, tn, 0);
@@ -1420,8 +1272,6 @@ int lbm_resident_ctas(int storage, int parity, int f16_round) {
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF16C, 1, 0, false>, kTile, 0);
     else if (storage == kStoreF16 && parity == 0)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF16, 0, 0, false>, kTile, 0);
-    else if (storage == kStoreF16)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF16, 1, 0, false>, kTile, 0);
     else
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, lbm_substep_kernel<kStoreF32, 1, 0, false>, kTile, 0);
     return max(1, sms * max(1, per_sm));
