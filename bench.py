@@ -309,7 +309,17 @@ def timed_steps(s, K, warmup, world, it0=0):
     return sum(a.elapsed_time(b) for a, b in ev), it, clk
 
 
-def substep_roofline(s, storage, it, l2):
+def pattern_peak(storage):
+    """The substep kernel's access pattern without the collision on this
+    workload's lattice and element size (glsm_pattern_bandwidth): the even and
+    odd forms' GB/s and their harmonic mean (the substeps alternate)."""
+    from glsm_fluid_3d_b200 import pattern_bandwidth
+
+    ge, go = pattern_bandwidth(DIMS, "f32" if storage == "f32" else "f16", 20)
+    return {"even": round(ge, 1), "odd": round(go, 1), "mean": round(2.0 / (1.0 / ge + 1.0 / go), 1)}
+
+
+def substep_roofline(s, storage, it, l2, pattern=None):
     """Achieved bandwidth of the substep kernel: graphs of one and of two velocity
     steps (nsub and 2 nsub substep launches) timed with one event pair each on
     the system stream; their difference over nsub is the launch time without
@@ -341,6 +351,11 @@ def substep_roofline(s, storage, it, l2):
             "l2_peak": round(l2, 1), "frac_l2": round(achieved / l2, 4),
             "l2_peak_how": f"glsm_copy_bandwidth: 2 x {L2_PROBE_BYTES >> 20} MiB copied back and forth "
                            f"{L2_PROBE_REPS} times in one launch, L1 bypassed (measured in this run)",
+            "pattern_peak": pattern["mean"] if pattern else None,
+            "frac_pattern": round(achieved / pattern["mean"], 4) if pattern else None,
+            "pattern_peak_how": ("glsm_pattern_bandwidth: the substep's 19-plane in-place read and write without the "
+                                 f"collision on this lattice, even {pattern['even']} / odd {pattern['odd']} GB/s, "
+                                 "harmonic mean (measured in this run, no L2 window)") if pattern else None,
             "kernel": "lbm_substep_kernel", "bytes_per_launch": bpc * N, "avg_launch_ms": round(avg_ms, 5),
             "avg_launch_ms_one_graph": round(st.median(one) / NSUB, 5),
             "avg_launch_ms_event_pairs": round(st.mean(prof), 5),
@@ -369,6 +384,7 @@ def run_ours(args, world, rank, local):
     from glsm_fluid_3d_b200 import copy_bandwidth
 
     l2 = copy_bandwidth(L2_PROBE_BYTES, L2_PROBE_REPS)
+    pattern = pattern_peak(args.storage)
     s = make_system(args.storage)
     fluid = s.fluid
     fluid.set_l2_persisting(not args.no_l2_persisting)  # one system alone on the GPU
@@ -380,7 +396,7 @@ def run_ours(args, world, rank, local):
 
     # dominant kernel: the substep kernel, timed as it runs inside the fused
     # iteration (graphs of its launches on the system stream)
-    roof, it = substep_roofline(s, args.storage, it, l2)
+    roof, it = substep_roofline(s, args.storage, it, l2, pattern)
 
     # end to end through the C ABI with host buffers: restart the state from
     # pinned host memory, run K iterations reading the gels' node velocities back
@@ -467,17 +483,19 @@ def f16_forms(args, f32_value, l2):
     out = {}
     N = DIMS[0] * DIMS[1] * DIMS[2]
     K = max(1, min(args.steps, args.f16_steps))
+    pattern = pattern_peak("f16")
     for storage in ("f16", "f16c"):
         s = make_system(storage)
         s.fluid.set_l2_persisting(not args.no_l2_persisting)
         t_ms, it, clk = timed_steps(s, K, args.warmup, 1)
-        roof, it = substep_roofline(s, storage, it, l2)
+        roof, it = substep_roofline(s, storage, it, l2, pattern)
         s.close()
         v = job_value(N, NSUB, K, 1, t_ms / 1e3)
         out[storage] = {"value": round(v, 1), "unit": "MLUPS", "steps": K, "ms_per_step": round(t_ms / K, 4),
                         "vs_f32": round(v / f32_value, 3),
                         "roofline": {k: roof[k] for k in ("achieved", "peak", "unit", "frac", "l2_peak", "frac_l2",
-                                                          "bytes_per_launch", "avg_launch_ms", "traffic")},
+                                                          "pattern_peak", "frac_pattern", "bytes_per_launch",
+                                                          "avg_launch_ms", "traffic")},
                         "clocks": clk}
     out["note"] = ("FP16 deviations f_q - w_q scaled by 2^20, FP32 collision; f16 rounds to nearest, f16c with the "
                    "mass- and momentum-conserving rounding; same workload, L2 flush and timing as the headline")

@@ -28,7 +28,7 @@ import numpy as np
 from ._lib import FluidDesc, GlsmError, check, lib
 
 __all__ = ["Gel", "Coupler", "Fluid", "System", "Batch", "GlsmError", "STORAGE", "lib", "copy_bandwidth",
-           "l2_reset_persisting", "l2_persisting_setaside"]
+           "pattern_bandwidth", "l2_reset_persisting", "l2_persisting_setaside"]
 
 STORAGE = {"f32": 0, "fp32": 0, "f16": 1, "fp16": 1, "bf16": 2, "f16c": 1, "f16c2": 1}
 # FP16 rounding modes (glsm_fluid_set_f16_rounding); storage "f16c" is FP16
@@ -70,6 +70,21 @@ def copy_bandwidth(nbytes: int, reps: int) -> float:
     if rc != 0:
         raise GlsmError(f"copy_bandwidth: {L.glsm_copy_bandwidth_error().decode()}")
     return out.value
+
+
+def pattern_bandwidth(dims, storage="f32", reps: int = 20):
+    """(even, odd) GB/s of the substep kernel's access pattern without the
+    collision on a lattice of `dims` in the kernel's layout and element size:
+    every cell reads its 19 populations and writes them back, in the even AA
+    form (own slots) and the odd form (neighbours' slots) (glsm_pattern_bandwidth)."""
+    L = lib()
+    ge, go = ctypes.c_double(0.0), ctypes.c_double(0.0)
+    st = STORAGE[storage] if isinstance(storage, str) else int(storage)
+    rc = L.glsm_pattern_bandwidth(int(dims[0]), int(dims[1]), int(dims[2]), st, int(reps), ctypes.byref(ge),
+                                  ctypes.byref(go))
+    if rc != 0:
+        raise GlsmError(f"pattern_bandwidth: {L.glsm_copy_bandwidth_error().decode()}")
+    return ge.value, go.value
 
 
 def _dptr(a):

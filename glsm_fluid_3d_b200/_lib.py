@@ -106,6 +106,7 @@ def lib():
     L.glsm_coupler_stream.argtypes = [vp]
     L.glsm_coupler_stream.restype = vp
     L.glsm_copy_bandwidth.argtypes = [ctypes.c_size_t, i, P(d)]
+    L.glsm_pattern_bandwidth.argtypes = [i, i, i, i, i, P(d), P(d)]
     L.glsm_copy_bandwidth.restype = i
     L.glsm_copy_bandwidth_error.restype = ctypes.c_char_p
     _lib = L

@@ -8,13 +8,62 @@
 // after the first is served by L2, with a footprint well above it by HBM.
 // Loads and stores go through L2 only (ld.global.cg / st.global.cg), so L1
 // never serves a re-read.
+//
+// A second probe measures the ceiling of the substep kernel's own access
+// pattern: every cell of a lattice reads its 19 populations and writes them
+// back with nothing computed in between, in the even AA form (the cell's own
+// slots, written to the opposite direction's plane) and in the odd form
+// (gathered from the 18 neighbours' slots, scattered back to them), with the
+// substep kernel's layout (19 planes, one per direction) and element size.
+// One population array, 19 read and 19 write streams: what a collision-free
+// substep could reach on this device.
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include <cstdio>
 
 #include "glsm_b200.h"
+#include "d3q19.cuh"
 
 namespace {
+
+using glsm::qcx;
+using glsm::qcy;
+using glsm::qcz;
+using glsm::qopp;
+
+// even AA form without the collision: cell i moves slot q to slot opp(q)
+template <typename T>
+__global__ void __launch_bounds__(256) aa_even_probe_kernel(T* P, unsigned n, size_t S) {
+    const unsigned i = blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    T v[19];
+#pragma unroll
+    for (int q = 0; q < 19; q++) v[q] = P[q * S + i];
+#pragma unroll
+    for (int q = 0; q < 19; q++) P[qopp(q) * S + i] = v[q];
+}
+
+// odd AA form without the collision, for the cells whose 18 neighbours lie
+// inside the array ([lo, hi)): gather slot opp(q) at i - off_q, scatter to
+// slot q at i + off_q
+template <typename T>
+__global__ void __launch_bounds__(256) aa_odd_probe_kernel(T* P, unsigned lo, unsigned hi, size_t S, int nx,
+                                                           int nxy) {
+    const unsigned i = lo + blockIdx.x * 256 + threadIdx.x;
+    if (i >= hi) return;
+    T v[19];
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        const int off = qcx(q) + qcy(q) * nx + qcz(q) * nxy;
+        v[q] = P[qopp(q) * S + i - off];
+    }
+#pragma unroll
+    for (int q = 0; q < 19; q++) {
+        const int off = qcx(q) + qcy(q) * nx + qcz(q) * nxy;
+        P[q * S + i + off] = v[q];
+    }
+}
 
 // Every thread copies the same elements in every rep, so a rep reads only what
 // the same thread wrote in the rep before: no synchronisation between threads.
@@ -44,6 +93,48 @@ thread_local char g_err[256];
 int bw_fail(const char* what, cudaError_t e) {
     snprintf(g_err, sizeof g_err, "%s: %s", what, e == cudaSuccess ? "bad argument" : cudaGetErrorString(e));
     return e == cudaSuccess ? GLSM_ERR_ARG : GLSM_ERR_CUDA;
+}
+
+template <typename T>
+int pattern_probe(int nx, int ny, int nz, int reps, double* gbs_even, double* gbs_odd) {
+    const unsigned n = (unsigned)nx * ny * nz, nxy = (unsigned)nx * ny;
+    const size_t S = ((size_t)n + 63) / 64 * 64, bytes = 19 * S * sizeof(T);
+    const unsigned lo = nxy + nx + 1, hi = n - nxy - nx - 1;
+    T* P = nullptr;
+    cudaStream_t s = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaError_t e = cudaMalloc(&P, bytes);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    for (int k = 0; k < 4 && e == cudaSuccess; k++) e = cudaEventCreate(&ev[k]);
+    if (e == cudaSuccess) e = cudaMemsetAsync(P, 0, bytes, s);
+    const unsigned ge = (n + 255) / 256, go = (hi - lo + 255) / 256;
+    auto even = [&] { aa_even_probe_kernel<T><<<ge, 256, 0, s>>>(P, n, S); };
+    auto odd = [&] { aa_odd_probe_kernel<T><<<go, 256, 0, s>>>(P, lo, hi, S, nx, (int)nxy); };
+    for (int k = 0; k < 4 && e == cudaSuccess; k++) {  // warm-up: the array into L2 where it fits
+        even();
+        odd();
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ev[0], s);
+    for (int k = 0; k < reps && e == cudaSuccess; k++) even();
+    if (e == cudaSuccess) e = cudaEventRecord(ev[1], s);
+    if (e == cudaSuccess) e = cudaEventRecord(ev[2], s);
+    for (int k = 0; k < reps && e == cudaSuccess; k++) odd();
+    if (e == cudaSuccess) e = cudaEventRecord(ev[3], s);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    float ms_even = 0.f, ms_odd = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms_even, ev[0], ev[1]);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms_odd, ev[2], ev[3]);
+    for (auto& x : ev)
+        if (x) cudaEventDestroy(x);
+    if (s) cudaStreamDestroy(s);
+    if (P) cudaFree(P);
+    if (e != cudaSuccess) return bw_fail("pattern probe", e);
+    const double per_cell = 2.0 * 19.0 * sizeof(T);
+    *gbs_even = (double)reps * n * per_cell / ((double)ms_even * 1e-3) / 1e9;
+    *gbs_odd = (double)reps * (hi - lo) * per_cell / ((double)ms_odd * 1e-3) / 1e9;
+    return GLSM_OK;
 }
 
 }  // namespace
@@ -94,6 +185,16 @@ int glsm_copy_bandwidth(size_t bytes, int reps, double* gbs) {
     if (e != cudaSuccess) return bw_fail("copy probe", e);
     *gbs = (double)reps * 2.0 * (double)bytes / ((double)ms * 1e-3) / 1e9;
     return GLSM_OK;
+}
+
+int glsm_pattern_bandwidth(int nx, int ny, int nz, int storage, int reps, double* gbs_even, double* gbs_odd) {
+    if (!gbs_even || !gbs_odd || nx < 4 || ny < 4 || nz < 4 || reps < 1 || reps > 10000 ||
+        (long long)nx * ny * nz > 200000000LL || storage < GLSM_STORE_F32 || storage > GLSM_STORE_BF16)
+        return bw_fail("glsm_pattern_bandwidth: lattice >= 4 per axis and <= 2e8 cells, storage 0-2, reps in [1, 10000]",
+                       cudaSuccess);
+    // 16-bit storages share one element size
+    return storage == GLSM_STORE_F32 ? pattern_probe<float>(nx, ny, nz, reps, gbs_even, gbs_odd)
+                                     : pattern_probe<__half>(nx, ny, nz, reps, gbs_even, gbs_odd);
 }
 
 }  // extern "C"

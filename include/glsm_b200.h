@@ -313,6 +313,18 @@ int glsm_fluid_units(glsm_fluid f, float out[2]);
  * reps in [1, 100000].  glsm_copy_bandwidth_error() explains a failure. */
 int glsm_copy_bandwidth(size_t bytes, int reps, double* gbs);
 const char* glsm_copy_bandwidth_error(void);
+/* Access-pattern probe (extension, a measurement aid with no counterpart in the
+ * reference): on an nx x ny x nz lattice in the substep kernel's layout and
+ * element size (storage GLSM_STORE_*), every cell reads its 19 populations and
+ * writes them back with no collision in between -- in the even AA form (own
+ * slots) and in the odd form (the 18 neighbours' slots, for the cells whose
+ * neighbours all lie in the array) -- `reps` launches each after a warm-up.
+ * *gbs_even / *gbs_odd receive 2 x 19 x element bytes per cell and launch
+ * over the time: the bandwidth a collision-free substep could reach with this
+ * pattern on this device, the roofline the substep kernel is set against
+ * beside the copy probes.  Allocates and frees its array; error text from
+ * glsm_copy_bandwidth_error(). */
+int glsm_pattern_bandwidth(int nx, int ny, int nz, int storage, int reps, double* gbs_even, double* gbs_odd);
 
 /* ---- Batch: several systems advanced together -----------------------------
  * No single counterpart in the reference (which runs one system per process);
