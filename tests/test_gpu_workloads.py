@@ -94,7 +94,7 @@ def test_full_size_rod_array_vs_oracle(gpu):
     bad = []
     for k in want:
         e = rel_l2(got[k], want[k])
-        t = {"u": 2e-5, "c1": 5e-6}.get(k, 1e-10)
+        t = {"u": 2e-5, "c1": 1e-5}.get(k, 1e-10)  # c1 as in the golden-case parity tests
         if not k.startswith("g") or k.split("_")[0] in ("g0", "g17", "g35"):  # the lattice and three rods
             print(f"L-full/5 {k:10s} rel_l2={e:.2e} tol={t:.0e}")
         if not e <= t:
