@@ -47,6 +47,22 @@ static int fail(int code, const char* fmt, ...) {
 struct glsm_coupler_s;
 struct glsm_fluid_s;
 
+// Output snapshot of an object (glsm_fluid_snapshot, glsm_gel_snapshot): the
+// fields are copied into `dev` on the object's stream, then to the caller's
+// host buffers on the copy stream, so the caller's thread never waits for the
+// iterations queued before the snapshot.
+struct Snapshot {
+    void* dev = nullptr;
+    size_t bytes = 0;
+    cudaStream_t copy = nullptr;
+    cudaEvent_t taken = nullptr;  // device-side copy done (recorded on the object's stream)
+    cudaEvent_t done = nullptr;   // host buffers filled (recorded on the copy stream)
+    bool used = false;            // a snapshot was taken: the next one waits for `done` on the device
+};
+
+static int snap_ensure(Snapshot& sn, size_t bytes);
+static void snap_release(Snapshot& sn);
+
 struct glsm_gel_s {
     GelDev d{};                 // descriptor with device pointers (host copy)
     GelDev* d_self = nullptr;   // device copy for launches before coupling
@@ -58,6 +74,7 @@ struct glsm_gel_s {
     glsm_coupler_s* coupler = nullptr;
     int index = -1;             // position in the coupler
     bool release_with_coupler = false;  // destroyed while coupled: freed with the coupler
+    Snapshot snap;              // output snapshot (glsm_gel_snapshot)
 };
 
 struct glsm_coupler_s {
@@ -95,6 +112,7 @@ struct glsm_fluid_s {
     double* d_cons = nullptr;    // conservation partial sums (kConsBlocks x 4) and result (4)
     struct glsm_batch_s* batch = nullptr;  // batch this system belongs to
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
+    Snapshot snap;               // output snapshot (glsm_fluid_snapshot)
 };
 
 // ---------------------------------------------------------------------------
@@ -167,8 +185,37 @@ static FieldRef gel_field(const glsm_gel_s* g, int field) {
         case GLSM_GEL_WMP: return {d.wmp, nE};
         case GLSM_GEL_FN_ROBIN: return {d.Fn_robin, 3 * nN};
         case GLSM_GEL_RM_LOC: return {d.rm_loc, 24 * nE};
+        case GLSM_GEL_SERIES: return {d.series, 12 * (size_t)d.series_cap};
         default: return {nullptr, 0};
     }
+}
+
+static int snap_ensure(Snapshot& sn, size_t bytes) {
+    if (!sn.copy) {
+        CK(cudaStreamCreateWithFlags(&sn.copy, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&sn.taken, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&sn.done, cudaEventDisableTiming));
+    }
+    if (bytes > sn.bytes) {
+        if (sn.dev) {
+            CK(cudaEventSynchronize(sn.done));
+            CK(cudaFree(sn.dev));
+            sn.dev = nullptr;
+            sn.bytes = 0;
+        }
+        CK(cudaMalloc(&sn.dev, bytes));
+        sn.bytes = bytes;
+    }
+    return GLSM_OK;
+}
+
+static void snap_release(Snapshot& sn) {
+    if (sn.copy) cudaStreamSynchronize(sn.copy);
+    if (sn.dev) cudaFree(sn.dev);
+    if (sn.taken) cudaEventDestroy(sn.taken);
+    if (sn.done) cudaEventDestroy(sn.done);
+    if (sn.copy) cudaStreamDestroy(sn.copy);
+    sn = Snapshot{};
 }
 
 // steady state of the BZ kinetics at w = FA0 by bisection on v
@@ -319,6 +366,7 @@ int glsm_gel_create(int sx, int sy, int sz, double px, double py, double pz, int
 }
 
 static void gel_release(glsm_gel g) {
+    snap_release(g->snap);
     cudaStreamSynchronize(g->own);
     cudaStreamDestroy(g->own);
     if (g->series_extra) cudaFree(g->series_extra);
@@ -417,6 +465,44 @@ int glsm_gel_read(glsm_gel g, int field, double* dst, size_t count) {
     if (count < f.count) return fail(GLSM_ERR_ARG, "field %d needs %zu doubles", field, f.count);
     CK(cudaMemcpyAsync(dst, f.ptr, f.count * sizeof(double), cudaMemcpyDeviceToHost, gel_stream(g)));
     CK(cudaStreamSynchronize(gel_stream(g)));
+    return GLSM_OK;
+}
+
+int glsm_gel_snapshot(glsm_gel g, int n_fields, const int* fields, double* const* dst) {
+    if (!g || n_fields < 1 || n_fields > 32 || !fields || !dst) return fail(GLSM_ERR_ARG, "bad snapshot arguments");
+    FieldRef f[32];
+    size_t total = 0;
+    for (int k = 0; k < n_fields; k++) {
+        f[k] = gel_field(g, fields[k]);
+        if (!f[k].ptr || !dst[k]) return fail(GLSM_ERR_ARG, "snapshot field %d: unknown field or null buffer", fields[k]);
+        total += f[k].count;
+    }
+    if (int r = snap_ensure(g->snap, total * sizeof(double))) return r;
+    Snapshot& sn = g->snap;
+    cudaStream_t s = gel_stream(g);
+    // the previous snapshot's transfer reads the device copy: overwrite it after
+    if (sn.used) CK(cudaStreamWaitEvent(s, sn.done, 0));
+    double* dev = static_cast<double*>(sn.dev);
+    size_t off = 0;
+    for (int k = 0; k < n_fields; k++) {
+        CK(cudaMemcpyAsync(dev + off, f[k].ptr, f[k].count * sizeof(double), cudaMemcpyDeviceToDevice, s));
+        off += f[k].count;
+    }
+    CK(cudaEventRecord(sn.taken, s));
+    CK(cudaStreamWaitEvent(sn.copy, sn.taken, 0));
+    off = 0;
+    for (int k = 0; k < n_fields; k++) {
+        CK(cudaMemcpyAsync(dst[k], dev + off, f[k].count * sizeof(double), cudaMemcpyDeviceToHost, sn.copy));
+        off += f[k].count;
+    }
+    CK(cudaEventRecord(sn.done, sn.copy));
+    sn.used = true;
+    return GLSM_OK;
+}
+
+int glsm_gel_snapshot_wait(glsm_gel g) {
+    if (!g) return fail(GLSM_ERR_ARG, "null gel");
+    if (g->snap.used) CK(cudaEventSynchronize(g->snap.done));
     return GLSM_OK;
 }
 
@@ -1026,6 +1112,7 @@ int glsm_fluid_destroy(glsm_fluid f) {
         for (auto& g : row)
             if (g) cudaGraphExecDestroy(g);
     if (f->scratch) cudaFree(f->scratch);
+    snap_release(f->snap);
     cudaFree(f->arena);
     f->c->fluid = nullptr;
     delete f;
@@ -1416,6 +1503,34 @@ int glsm_fluid_read(glsm_fluid f, int field, float* dst, size_t count) {
         default: return fail(GLSM_ERR_ARG, "unknown fluid field %d", field);
     }
     return glsm_fluid_sync(f);
+}
+
+int glsm_fluid_snapshot(glsm_fluid f, float* u_dst, float* c_dst) {
+    if (!f || !u_dst || !c_dst) return fail(GLSM_ERR_ARG, "null argument");
+    if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
+    const long long N = f->F.N;
+    if (int r = snap_ensure(f->snap, 4 * (size_t)N * sizeof(float))) return r;
+    Snapshot& sn = f->snap;
+    cudaStream_t s = f->c->stream;
+    if (sn.used) CK(cudaStreamWaitEvent(s, sn.done, 0));
+    float* dev_u = static_cast<float*>(sn.dev);
+    float* dev_c = dev_u + 3 * N;
+    u_pack_kernel<<<(unsigned)((N + 255) / 256), 256, 0, s>>>(f->F.u, N, dev_u, 1);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(dev_c, f->F.c[f->cur], N * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    CK(cudaEventRecord(sn.taken, s));
+    CK(cudaStreamWaitEvent(sn.copy, sn.taken, 0));
+    CK(cudaMemcpyAsync(u_dst, dev_u, 3 * N * sizeof(float), cudaMemcpyDeviceToHost, sn.copy));
+    CK(cudaMemcpyAsync(c_dst, dev_c, N * sizeof(float), cudaMemcpyDeviceToHost, sn.copy));
+    CK(cudaEventRecord(sn.done, sn.copy));
+    sn.used = true;
+    return GLSM_OK;
+}
+
+int glsm_fluid_snapshot_wait(glsm_fluid f) {
+    if (!f) return fail(GLSM_ERR_ARG, "null fluid");
+    if (f->snap.used) CK(cudaEventSynchronize(f->snap.done));
+    return GLSM_OK;
 }
 
 int glsm_fluid_write(glsm_fluid f, int field, const float* src, size_t count) {

@@ -88,6 +88,71 @@ void read_gel(glsm_gel h, int field, void* dst, size_t count) {
     check(glsm_gel_read(h, field, static_cast<double*>(dst), count), "read gel field");
 }
 
+// errors on a writer thread are reported, never thrown
+void report(int rc, const char* what) {
+    if (rc != GLSM_OK) std::fprintf(stderr, "glsm: %s: %s\n", what, glsm_last_error());
+}
+
+// the .dat files of one gel at `time` (Gel::recordData, src/gel.cu:452-541):
+// node fields rn, Fn, Veln over the interior nodes and element fields rm, um,
+// vm, wm over the interior elements, z slowest; the centre-element records of
+// iterations in ((time - 1) df, time df] appended to gel<id>bodycenter.dat
+// (columns of src/gel.cu:512-524)
+void write_gel_dat(int id, int time, int df, int3 grid, const double3* rn, const double3* Fn, const double3* Veln,
+                   const double3* rm, const double* um, const double* vm, const double* wm, const double* series,
+                   size_t n_records) {
+    const int LX = grid.x, LY = grid.y, LZ = grid.z;
+    auto gi = [&](int x, int y, int z, int size) { return x + y * (LX + size) + z * (LY + size) * (LX + size); };
+    const std::string sid = std::to_string(id), t = std::to_string(time);
+    std::vector<int> nodes, elems;
+    for (int zi = 1; zi < LZ + 1; zi++)
+        for (int yi = 1; yi < LY + 1; yi++)
+            for (int xi = 1; xi < LX + 1; xi++) nodes.push_back(gi(xi, yi, zi, 2));
+    for (int zi = 1; zi < LZ; zi++)
+        for (int yi = 1; yi < LY; yi++)
+            for (int xi = 1; xi < LX; xi++) elems.push_back(gi(xi, yi, zi, 1));
+    write_lines("gel" + sid + "rn" + t + ".dat", nodes.size(), [&](size_t i, std::string& o) { vec_line(rn[nodes[i]], o); });
+    write_lines("gel" + sid + "Fn" + t + ".dat", nodes.size(), [&](size_t i, std::string& o) { vec_line(Fn[nodes[i]], o); });
+    write_lines("gel" + sid + "Veln" + t + ".dat", nodes.size(),
+                [&](size_t i, std::string& o) { vec_line(Veln[nodes[i]], o); });
+    write_lines("gel" + sid + "rm" + t + ".dat", elems.size(), [&](size_t i, std::string& o) { vec_line(rm[elems[i]], o); });
+    write_lines("gel" + sid + "um" + t + ".dat", elems.size(), [&](size_t i, std::string& o) {
+        o += fmt_fixed(um[elems[i]]);
+        o += '\n';
+    });
+    write_lines("gel" + sid + "vm" + t + ".dat", elems.size(), [&](size_t i, std::string& o) {
+        o += fmt_default(vm[elems[i]]);
+        o += '\n';
+    });
+    write_lines("gel" + sid + "wm" + t + ".dat", elems.size(), [&](size_t i, std::string& o) {
+        o += fmt_default(wm[elems[i]]);
+        o += '\n';
+    });
+    std::ofstream bc("gel" + sid + "bodycenter.dat", std::ios::app);
+    for (size_t r = 0; r < n_records; r++) {
+        const double* rec = series + 12 * r;
+        if (rec[0] <= 0.0 || (int)rec[0] > time * df || (int)rec[0] <= (time - 1) * df) continue;
+        std::string line = fmt_fixed(rec[0]);
+        for (int k = 1; k < 12; k++) {
+            line += kSep;
+            line += fmt_fixed(rec[k]);
+        }
+        bc << line << "\n";
+    }
+}
+
+// Velb<t>.dat and Conc<t>.dat (Fluid::recordData, src/fluid.cu:115-138), x fastest
+void write_fluid_dat(int time, size_t N, const float* u, const float* c) {
+    const std::string t = std::to_string(time);
+    write_lines("Velb" + t + ".dat", N, [&](size_t i, std::string& o) {
+        vec_line(make_double3(u[3 * i], u[3 * i + 1], u[3 * i + 2]), o);
+    });
+    write_lines("Conc" + t + ".dat", N, [&](size_t i, std::string& o) {
+        o += fmt_fixed(c[i]);
+        o += '\n';
+    });
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -184,6 +249,7 @@ Gel::Gel(int3 gelSize, double3 gelPosition, int gelType, int gel_id, int time)
 
 Gel::~Gel() {
     if (m_file_writer_thread.joinable()) m_file_writer_thread.join();
+    if (m_snap) cudaFreeHost(m_snap);
     check(glsm_gel_destroy(handle), "~Gel");
     delete[] m_hum;
     delete[] m_hvm;
@@ -245,57 +311,55 @@ void Gel::copyDataToDevice() {
     check(glsm_gel_write(handle, GLSM_GEL_RN, (double*)m_hrn, 3 * (size_t)m_numGelNodes), "write rn");
 }
 
-// Gel::recordData, src/gel.cu:452-541: node fields rn, Fn, Veln over the interior
-// nodes and element fields rm, um, vm, wm over the interior elements, z slowest.
-// The centre-element series is appended to gel<id>bodycenter.dat, one line per
-// recorded iteration (columns of src/gel.cu:512-524).
+// Gel::recordData, src/gel.cu:452-541: the .dat files of the host mirrors
+// (filled by copyDataToHost)
 void Gel::recordData(int time) {
-    const int LX = m_gelNodeGrid.x, LY = m_gelNodeGrid.y, LZ = m_gelNodeGrid.z;
-    const std::string id = std::to_string(m_gelId), t = std::to_string(time);
-    std::vector<int> nodes, elems;
-    for (int zi = 1; zi < LZ + 1; zi++)
-        for (int yi = 1; yi < LY + 1; yi++)
-            for (int xi = 1; xi < LX + 1; xi++) nodes.push_back(get_index(xi, yi, zi, 2));
-    for (int zi = 1; zi < LZ; zi++)
-        for (int yi = 1; yi < LY; yi++)
-            for (int xi = 1; xi < LX; xi++) elems.push_back(get_index(xi, yi, zi, 1));
-    write_lines("gel" + id + "rn" + t + ".dat", nodes.size(), [&](size_t i, std::string& o) { vec_line(m_hrn[nodes[i]], o); });
-    write_lines("gel" + id + "Fn" + t + ".dat", nodes.size(), [&](size_t i, std::string& o) { vec_line(m_hFn[nodes[i]], o); });
-    write_lines("gel" + id + "Veln" + t + ".dat", nodes.size(), [&](size_t i, std::string& o) { vec_line(m_hVeln[nodes[i]], o); });
-    write_lines("gel" + id + "rm" + t + ".dat", elems.size(), [&](size_t i, std::string& o) { vec_line(m_hrm[elems[i]], o); });
-    write_lines("gel" + id + "um" + t + ".dat", elems.size(), [&](size_t i, std::string& o) {
-        o += fmt_fixed(m_hum[elems[i]]);
-        o += '\n';
-    });
-    write_lines("gel" + id + "vm" + t + ".dat", elems.size(), [&](size_t i, std::string& o) {
-        o += fmt_default(m_hvm[elems[i]]);
-        o += '\n';
-    });
-    write_lines("gel" + id + "wm" + t + ".dat", elems.size(), [&](size_t i, std::string& o) {
-        o += fmt_default(m_hwm[elems[i]]);
-        o += '\n';
-    });
-    std::ofstream bc("gel" + id + "bodycenter.dat", std::ios::app);
-    for (int r = 0; r < 1000; r++) {
-        const double* rec = m_hseries + 12 * r;
-        if (rec[0] <= 0.0 || (int)rec[0] > time * m_df || (int)rec[0] <= (time - 1) * m_df) continue;
-        std::string line = fmt_fixed(rec[0]);
-        for (int k = 1; k < 12; k++) {
-            line += kSep;
-            line += fmt_fixed(rec[k]);
-        }
-        bc << line << "\n";
-    }
+    write_gel_dat(m_gelId, time, m_df, m_gelNodeGrid, m_hrn, m_hFn, m_hVeln, m_hrm, m_hum, m_hvm, m_hwm, m_hseries,
+                  1000);
 }
 
-// Gel::writeFiles, src/gel.cu:543-553
+// Gel::writeFiles, src/gel.cu:543-553.  Where the reference copies the fields
+// to the host synchronously (waiting for every queued kernel) and formats them
+// on a writer thread, this takes an output snapshot -- a device-side copy
+// behind the queued work, then a transfer on a copy stream into page-locked
+// staging -- and returns at once; the writer thread waits for the transfer and
+// formats the staging.  The host mirrors are left as they are.
 void Gel::writeFiles(int iter) {
     const double time = iter * m_dt;
     if (iter % 1000 == 0) {
         if (m_file_writer_thread.joinable()) m_file_writer_thread.join();
-        copyDataToHost();
-        m_file_writer_thread = std::thread(&Gel::recordData, this, int(time));
+        const size_t nN3 = 3 * (size_t)m_numGelNodes, nE = m_numGelElements;
+        const size_t ns = glsm_gel_field_size(handle, GLSM_GEL_SERIES);
+        const size_t need = 3 * nN3 + 3 * nE + 3 * nE + ns;
+        if (need > m_snap_doubles) {
+            if (m_snap) cudaFreeHost(m_snap);
+            m_snap = nullptr;
+            m_snap_doubles = 0;
+            if (cudaMallocHost(&m_snap, need * sizeof(double)) != cudaSuccess) {
+                cudaGetLastError();
+                check(GLSM_ERR_NOMEM, "writeFiles: page-locked staging");
+                return;
+            }
+            m_snap_doubles = need;
+        }
+        double* const dst[8] = {m_snap, m_snap + nN3, m_snap + 2 * nN3, m_snap + 3 * nN3, m_snap + 3 * nN3 + 3 * nE,
+                                m_snap + 3 * nN3 + 4 * nE, m_snap + 3 * nN3 + 5 * nE, m_snap + 3 * nN3 + 6 * nE};
+        const int fields[8] = {GLSM_GEL_RN, GLSM_GEL_FN, GLSM_GEL_VELN, GLSM_GEL_RM,
+                               GLSM_GEL_UM, GLSM_GEL_VM, GLSM_GEL_WM, GLSM_GEL_SERIES};
+        check(glsm_gel_snapshot(handle, 8, fields, dst), "writeFiles: snapshot");
+        m_file_writer_thread = std::thread(&Gel::writeSnapshot, this, int(time));
     }
+}
+
+// writer thread of writeFiles: waits for the snapshot, formats the staging
+void Gel::writeSnapshot(int time) {
+    report(glsm_gel_snapshot_wait(handle), "writeFiles: snapshot");
+    const size_t nN3 = 3 * (size_t)m_numGelNodes, nE = m_numGelElements;
+    const double* p = m_snap;
+    write_gel_dat(m_gelId, time, m_df, m_gelNodeGrid, reinterpret_cast<const double3*>(p),
+                  reinterpret_cast<const double3*>(p + nN3), reinterpret_cast<const double3*>(p + 2 * nN3),
+                  reinterpret_cast<const double3*>(p + 3 * nN3), p + 3 * nN3 + 3 * nE, p + 3 * nN3 + 4 * nE,
+                  p + 3 * nN3 + 5 * nE, p + 3 * nN3 + 6 * nE, (m_snap_doubles - 3 * nN3 - 6 * nE) / 12);
 }
 
 // Gel::setGoonValue, src/gel.cu:221-282: restart from gel<id>{rn,um,vm,wm}<time>.dat
@@ -436,6 +500,7 @@ void Fluid::init(int3 dims, int nsub, int storage, int time) {
 
 Fluid::~Fluid() {
     if (file_writer_thread.joinable()) file_writer_thread.join();
+    if (m_snap_u) cudaFreeHost(m_snap_u);
     check(glsm_fluid_destroy(handle), "~Fluid");
     delete[] h_u;
     delete[] h_c1;
@@ -453,26 +518,35 @@ void Fluid::copyDataToHost() {
     check(glsm_fluid_read(handle, GLSM_FLUID_C1, h_c1, (size_t)N), "read c1");
 }
 
-// Fluid::recordData, src/fluid.cu:115-138: Velb<t>.dat and Conc<t>.dat, x fastest
-void Fluid::recordData(int time) {
-    const std::string t = std::to_string(time);
-    write_lines("Velb" + t + ".dat", (size_t)N, [&](size_t i, std::string& o) {
-        vec_line(make_double3(h_u[i].x, h_u[i].y, h_u[i].z), o);
-    });
-    write_lines("Conc" + t + ".dat", (size_t)N, [&](size_t i, std::string& o) {
-        o += fmt_fixed(h_c1[i]);
-        o += '\n';
-    });
-}
+// Fluid::recordData, src/fluid.cu:115-138: the .dat files of the host mirrors
+// (filled by copyDataToHost)
+void Fluid::recordData(int time) { write_fluid_dat(time, (size_t)N, reinterpret_cast<const float*>(h_u), h_c1); }
 
-// Fluid::writeFiles, src/fluid.cu:140-150
+// Fluid::writeFiles, src/fluid.cu:140-150, with an output snapshot as in
+// Gel::writeFiles: returns without waiting for the queued iterations; the
+// writer thread waits for the transfer and formats the staging
 void Fluid::writeFiles(int iter) {
     const double time = iter * dt;
     if (iter % 2000 == 0) {
         if (file_writer_thread.joinable()) file_writer_thread.join();
-        copyDataToHost();
-        file_writer_thread = std::thread(&Fluid::recordData, this, int(time));
+        if (!m_snap_u) {
+            if (cudaMallocHost(&m_snap_u, 4 * sizeof(float) * (size_t)N) != cudaSuccess) {
+                cudaGetLastError();
+                m_snap_u = nullptr;
+                check(GLSM_ERR_NOMEM, "writeFiles: page-locked staging");
+                return;
+            }
+            m_snap_c = m_snap_u + 3 * (size_t)N;
+        }
+        check(glsm_fluid_snapshot(handle, m_snap_u, m_snap_c), "writeFiles: snapshot");
+        file_writer_thread = std::thread(&Fluid::writeSnapshot, this, int(time));
     }
+}
+
+// writer thread of writeFiles: waits for the snapshot, formats the staging
+void Fluid::writeSnapshot(int time) {
+    report(glsm_fluid_snapshot_wait(handle), "writeFiles: snapshot");
+    write_fluid_dat(time, (size_t)N, m_snap_u, m_snap_c);
 }
 
 // Fluid::setGoonValue, src/fluid.cu:57-83: u and c1 from Velb<t>.dat / Conc<t>.dat,

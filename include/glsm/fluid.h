@@ -67,4 +67,9 @@ public:
 
 private:
     void init(int3 dims, int nsub, int storage, int time);
+    // page-locked staging of the output snapshot (u, c1) that writeFiles'
+    // writer thread formats
+    float* m_snap_u = nullptr;
+    float* m_snap_c = nullptr;
+    void writeSnapshot(int time);
 };

@@ -100,4 +100,11 @@ public:
     bool flag = false;
 
     glsm_gel handle;  // the library object
+
+private:
+    // page-locked staging of the output snapshot that writeFiles' writer
+    // thread formats (rn, Fn, Veln, rm, um, vm, wm, the time series)
+    double* m_snap = nullptr;
+    size_t m_snap_doubles = 0;
+    void writeSnapshot(int time);
 };

@@ -68,7 +68,10 @@ enum glsm_gel_field {
     GLSM_GEL_WMP = 19,     /* m_dwmp                                          */
     GLSM_GEL_FN_ROBIN = 20,/* m_dFn_robin                                     */
     GLSM_GEL_RM_LOC = 21,  /* m_drm_loc  (24 per element)                     */
-    GLSM_GEL_NFIELDS = 22
+    GLSM_GEL_NFIELDS = 22,
+    /* the centre-element time series (glsm_gel_series_config): 12 doubles per
+     * record x capacity, for glsm_gel_read / glsm_gel_field_size / snapshots */
+    GLSM_GEL_SERIES = 64
 };
 
 /* lattice fields for glsm_fluid_read / _write (FP32, reference layout) */
@@ -132,6 +135,14 @@ int glsm_gel_record_center(glsm_gel g, int iter);
  * of the centre element (the columns of gel<id>bodycenter.dat, gel.cu:505-537) */
 int glsm_gel_series_config(glsm_gel g, int every, int capacity);
 int glsm_gel_series_read(glsm_gel g, double* dst, size_t count);
+/* Output snapshot of gel fields (extension; Gel::copyDataToHost,
+ * src/gel.cu:355-373, is synchronous): fields[k] (GLSM_GEL_* fields, the
+ * time-series ring included) are copied on the device behind the queued work,
+ * then transferred into dst[k] on a copy stream; returns at once (as
+ * glsm_fluid_snapshot; dst page-locked and untouched until
+ * glsm_gel_snapshot_wait returns).  At most 32 fields. */
+int glsm_gel_snapshot(glsm_gel g, int n_fields, const int* fields, double* const* dst);
+int glsm_gel_snapshot_wait(glsm_gel g);
 /* Gel::resetToQuiescent(), src/gel.cu:731-747 */
 int glsm_gel_reset_quiescent(glsm_gel g);
 /* Gel::fireExcitationPulse(), src/gel.cu:751-783 */
@@ -221,6 +232,16 @@ int glsm_checkpoint_save(glsm_fluid f, void* buf, size_t bytes);
 int glsm_checkpoint_load(glsm_fluid f, const void* buf, size_t bytes);
 /* host copies of lattice fields (FP32, reference layout) */
 int glsm_fluid_read(glsm_fluid f, int field, float* dst, size_t count);
+/* Output snapshot (extension; Fluid::copyDataToHost, src/fluid.cu:85-90, is
+ * synchronous): enqueues behind the work already queued on the system stream a
+ * device-side copy of u (3 N floats, xyz) and of the current c1 (N floats),
+ * then their transfer into u_dst and c_dst on a copy stream, and returns at
+ * once.  Iterations enqueued afterwards run on without waiting for the transfer.
+ * For the transfer to overlap, u_dst and c_dst must be page-locked host memory
+ * (cudaMallocHost); they must stay untouched until glsm_fluid_snapshot_wait
+ * returns.  A later snapshot waits on the device for the earlier transfer. */
+int glsm_fluid_snapshot(glsm_fluid f, float* u_dst, float* c_dst);
+int glsm_fluid_snapshot_wait(glsm_fluid f);
 /* replace populations (GLSM_FLUID_POP, absolute values), u (GLSM_FLUID_U) or c1 */
 int glsm_fluid_write(glsm_fluid f, int field, const float* src, size_t count);
 /* Global mass and momentum of the lattice (extension; the reference computes

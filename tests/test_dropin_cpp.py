@@ -47,6 +47,31 @@ def test_reference_sim_cpp_compiles_unchanged(tmp_path):
 
 
 @pytest.mark.gpu
+def test_write_files_does_not_wait_for_the_device(gpu, tmp_path):
+    """Gel::writeFiles / Fluid::writeFiles return while the device still works
+    through 300 queued iterations of the 101^3 workload (an output snapshot
+    instead of a synchronous copy), and the files they write equal those of the
+    synchronous copyDataToHost + recordData of the same state."""
+    exe = str(tmp_path / "dat_async")
+    compile_driver(os.path.join(ROOT, "tests", "drivers", "dat_async.cpp"), exe)
+    env = dict(os.environ)
+    env.pop("IBM_BETA", None)
+    env.pop("IBM_RAMP_STEPS", None)
+    d = tmp_path / "out"
+    out = subprocess.run([exe, str(d)], capture_output=True, text=True, env=env, check=True).stdout
+    t = {k: float(v) for k, v in re.findall(r"(\w+_ms)=([\d.]+)", out)}
+    print(out.strip())
+    assert "N=1030301" in out
+    # the device had most of the 300 iterations (~0.6 ms each) still to run
+    # when the calls returned
+    assert t["drain_ms"] > 60.0, t
+    assert t["writefiles_ms"] < 0.25 * t["drain_ms"], t
+    for name in ["gel1rn", "gel1Fn", "gel1Veln", "gel1rm", "gel1um", "gel1vm", "gel1wm", "gel2rn", "gel2um",
+                 "Velb", "Conc"]:
+        assert open(d / f"{name}2.dat").read() == open(d / f"{name}3.dat").read(), name
+
+
+@pytest.mark.gpu
 def test_driver_matches_python_path(gpu, tmp_path):
     """The C++ driver and the Python per-method loop give the same gel state and
     the same .dat contents after 20 iterations."""
