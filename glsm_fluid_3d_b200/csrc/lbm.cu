@@ -534,8 +534,10 @@ __device__ __forceinline__ void store_u(const StepArgs& a, unsigned i, bool inb,
     if (inb || a.last) a.F.u[i] = u;
 }
 
-// force, collision and AA-pattern scatter of one cell
-template <int ST, int PARITY, int PERX>
+// force, collision and AA-pattern scatter of one cell; TAB: the launch's
+// per-direction base pointers (StepArgs::scatter) address the even and the
+// wall-free odd scatters
+template <int ST, int PARITY, int PERX, bool TAB>
 __device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, unsigned x, bool fast, bool xin,
                                                 bool inb, float (&d)[19]) {
     using IO = PopIO<ST>;
@@ -549,7 +551,10 @@ __device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, u
     if constexpr (IO::kConserve) conserve_round(d);
 
     T* Pi = P + i;
-    if (PARITY == 0) {
+    if (TAB && (PARITY == 0 || (fast && xin))) {
+#pragma unroll
+        for (int q = 0; q < 19; q++) IO::st_raw(reinterpret_cast<T*>(a.scatter[q]) + i, d[q]);
+    } else if (PARITY == 0) {
 #pragma unroll
         for (int q = 0; q < 19; q++) IO::st_raw(Pi + qopp(q) * LS, d[q]);
     } else if (fast && xin) {
@@ -611,8 +616,10 @@ __device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, u
 
 // one cell of a substep: gather (AA pattern), collide, scatter.  Addresses are a
 // per-thread base pointer (the cell in plane 0) plus per-direction offsets that
-// depend only on the lattice, the same for every lane.
-template <int ST, int PARITY, int PERX>
+// depend only on the lattice, the same for every lane; with TAB the even and
+// the wall-free odd accesses use the launch's per-direction base pointers
+// (StepArgs::gather / scatter) instead, one add per access.
+template <int ST, int PARITY, int PERX, bool TAB>
 __device__ __forceinline__ void lbm_cell(const StepArgs& a, unsigned i, bool inb) {
     using IO = PopIO<ST>;
     using T = typename IO::T;
@@ -635,7 +642,10 @@ __device__ __forceinline__ void lbm_cell(const StepArgs& a, unsigned i, bool inb
         fast = __all_sync(act, (y - 1u < ny - 2u) && (z - 1u < nz - 2u));
         xin = __all_sync(act, x - 1u < nx - 2u);
     }
-    if (PARITY == 0) {
+    if (TAB && (PARITY == 0 || (fast && xin))) {
+#pragma unroll
+        for (int q = 0; q < 19; q++) d[q] = IO::raw(reinterpret_cast<const T*>(a.gather[q]) + i);
+    } else if (PARITY == 0) {
 #pragma unroll
         for (int q = 0; q < 19; q++) d[q] = IO::raw(Pi + q * LS);
     } else if (fast && xin) {
@@ -693,7 +703,7 @@ __device__ __forceinline__ void lbm_cell(const StepArgs& a, unsigned i, bool inb
             d[q] = IO::raw(P + (wall ? q * S + i : qopp(q) * S + i + (unsigned)off));
         }
     }
-    collide_scatter<ST, PARITY, PERX>(a, i, x, fast, xin, inb, d);
+    collide_scatter<ST, PARITY, PERX, TAB>(a, i, x, fast, xin, inb, d);
 }
 
 // Per-tile state prepared by warp 0 one tile ahead: the ticket and the marker
@@ -751,7 +761,7 @@ __device__ __forceinline__ void prepare_slot(const StepArgs& a, unsigned t, Tile
 // even substep of two adjacent cells i0 (even) and i0 + 1: one vector load and
 // one vector store per direction, the pair's populations staying packed in
 // registers while each cell collides in turn
-template <int ST>
+template <int ST, bool TAB>
 __device__ __forceinline__ void lbm_pair_even(const StepArgs& a, unsigned i0, bool inb0, bool inb1) {
     using PIO = PairIO<ST>;
     using V = typename PIO::V;
@@ -760,7 +770,8 @@ __device__ __forceinline__ void lbm_pair_even(const StepArgs& a, unsigned i0, bo
     V* Pv = reinterpret_cast<V*>(F.pop) + (i0 >> 1);
     V r[19];
 #pragma unroll
-    for (int q = 0; q < 19; q++) r[q] = Pv[q * LS2];
+    for (int q = 0; q < 19; q++)
+        r[q] = TAB ? reinterpret_cast<const V*>(a.gather[q])[i0 >> 1] : Pv[q * LS2];
     {
         float d[19];
 #pragma unroll
@@ -781,7 +792,12 @@ __device__ __forceinline__ void lbm_pair_even(const StepArgs& a, unsigned i0, bo
     }
     // post-collision f_q goes to the cell's own slot opp(q)
 #pragma unroll
-    for (int q = 0; q < 19; q++) Pv[qopp(q) * LS2] = r[q];
+    for (int q = 0; q < 19; q++) {
+        if (TAB)
+            reinterpret_cast<V*>(a.scatter[q])[i0 >> 1] = r[q];
+        else
+            Pv[qopp(q) * LS2] = r[q];
+    }
 }
 
 // whether cell i lies in a marker box of the tile; with deterministic spreads a
@@ -810,7 +826,7 @@ __device__ __forceinline__ bool in_boxes(const StepArgs& a, const TileSlot& sl, 
 
 // a lattice tile of consecutive cells (tile_range), up to kCellsPerThread per
 // thread: adjacent pairs on even substeps of FP16 storage, else cells kTile apart
-template <int ST, int PARITY, int PERX, bool PAIR = false, bool DET = false>
+template <int ST, int PARITY, int PERX, bool PAIR = false, bool DET = false, bool TAB = false>
 __device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const TileSlot& sl) {
     unsigned c0, c1;
     tile_range(a, tile, c0, c1);
@@ -821,15 +837,15 @@ __device__ __forceinline__ void lbm_tile(const StepArgs& a, unsigned tile, const
         const bool inb0 = nb > 0 && i0 <= c1 && in_boxes<DET>(a, sl, nb, i0);
         const bool inb1 = nb > 0 && i0 + 1 <= c1 && in_boxes<DET>(a, sl, nb, i0 + 1);
         if (i0 + 1 <= c1) {
-            lbm_pair_even<ST>(a, i0, inb0, inb1);
+            lbm_pair_even<ST, TAB>(a, i0, inb0, inb1);
         } else if (i0 <= c1) {
-            lbm_cell<ST, PARITY, PERX>(a, i0, inb0);
+            lbm_cell<ST, PARITY, PERX, TAB>(a, i0, inb0);
         }
     } else {
 #pragma unroll 1
         for (int r = 0; r < kCellsPerThread; r++) {
             const unsigned i = c0 + r * kTile + threadIdx.x;
-            if (i <= c1) lbm_cell<ST, PARITY, PERX>(a, i, nb > 0 && in_boxes<DET>(a, sl, nb, i));
+            if (i <= c1) lbm_cell<ST, PARITY, PERX, TAB>(a, i, nb > 0 && in_boxes<DET>(a, sl, nb, i));
         }
     }
 }
@@ -875,7 +891,7 @@ __global__ void __launch_bounds__(kTile, (lbm_ctas_per_sm<ST, PARITY>())) lbm_su
         if (t < (unsigned)a.n_ibm)
             ibm_task(a, t);
         else
-            lbm_tile<ST, PARITY, PERX, true, DET>(a, t - a.n_ibm, s_slot[j]);
+            lbm_tile<ST, PARITY, PERX, true, DET, true>(a, t - a.n_ibm, s_slot[j]);
         if (warp0) {
             tn = __shfl_sync(0xffffffffu, tn, 0);
             prepare_slot(a, tn, s_slot[j ^ 1]);
@@ -1277,7 +1293,22 @@ int lbm_resident_ctas(int storage, int parity, int f16_round) {
     return max(1, sms * max(1, per_sm));
 }
 
-cudaError_t launch_substep(const StepArgs& a, int parity, cudaStream_t s) {
+cudaError_t launch_substep(const StepArgs& a_in, int parity, cudaStream_t s) {
+    StepArgs a = a_in;
+    {
+        // the per-direction base pointers of this parity (element offsets from
+        // the population array; odd: shifted by the neighbour offset)
+        const size_t esz = a.F.storage == kStoreF32 ? 4 : 2;
+        char* P = static_cast<char*>(a.F.pop);
+        const long long S = a.F.S, nx = a.F.nx, nxy = (long long)a.F.nx * a.F.ny;
+        for (int q = 0; q < 19; q++) {
+            const long long off = qcx(q) + qcy(q) * nx + qcz(q) * nxy;
+            const long long g = parity ? qopp(q) * S - off : q * S;
+            const long long w = parity ? q * S + off : qopp(q) * S;
+            a.gather[q] = P + g * (long long)esz;
+            a.scatter[q] = P + w * (long long)esz;
+        }
+    }
     dim3 grid(lbm_grid(a, parity)), block(kTile);
     // substeps after the first are launched with programmatic stream
     // serialization (the kernel waits for its predecessor itself,

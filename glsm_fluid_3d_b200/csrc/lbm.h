@@ -23,6 +23,13 @@ struct StepArgs {
     int lbm_ctas_even;   // persistent CTAs per even-substep launch (0: one per ticket)
     int wait_extra;      // test aid: IBM tasks a force-region tile waits for beyond n_ibm (> 0 makes the
                          // bounded wait run out; 0 in every normal launch)
+    // Per-direction base pointers of this launch's substep parity, set by
+    // launch_substep: the cell i's value of direction q is read at gather[q] + i
+    // and written at scatter[q] + i (even: slots q and opp(q) of the cell; odd,
+    // away from walls: slot opp(q) of the upstream neighbour, slot q of the
+    // downstream one).  Unused (null) in batched launches.
+    const void* gather[19];
+    void* scatter[19];
     float l2_hit;        // > 0: substep launches mark the first l2_bytes of the population
     unsigned long long l2_bytes;  // array L2-persisting with this hit ratio
 };
