@@ -145,7 +145,7 @@ def ncu_traffic(storage):
     try:
         for line in open(path):
             if line.startswith("dram_bytes_per_launch:"):
-                return float(line.split(":")[1])
+                return float(line.split(":")[1].split()[0])
     except OSError:
         pass
     return None
