@@ -137,10 +137,11 @@ class Stats:
 class Server:
     """Admits requests by HBM budget and advances all resident systems together.
 
-    Each round launches a chunk of batched iterations and, while it runs on the
-    device, builds the systems of the requests that have arrived (as far as the
-    budget allows); after the chunk it retires finished systems (reading their
-    results) and adds the newly built ones to the batch."""
+    Each round launches a chunk of batched iterations -- up to the iteration at
+    which the first member completes, at most max_chunk -- and, while it runs
+    on the device, builds the systems of the requests that have arrived (as far
+    as the budget allows); after the chunk it retires the finished systems
+    (reading their results) and adds the newly built ones to the batch."""
 
     def __init__(self, budget_bytes: float = 150e9, max_chunk: int = 20, keep_results: bool = False):
         self.budget = budget_bytes
@@ -179,8 +180,10 @@ class Server:
                     if not built and pending:  # idle until the next arrival
                         time.sleep(max(0.0, pending[0].arrival - (clock() - t0)))
                     continue
-                # a fixed chunk: members that finish inside it idle until it ends
-                chunk = min(self.max_chunk, max(v[2] for v in active.values()))
+                # the chunk ends when the first member finishes (or after
+                # max_chunk iterations, so that arrivals join soon): no member
+                # idles inside a chunk, and each is retired the moment it is done
+                chunk = min(self.max_chunk, min(v[2] for v in active.values()))
                 batch.run(chunk)
                 admit()  # overlaps the chunk running on the device
                 tw = clock()
