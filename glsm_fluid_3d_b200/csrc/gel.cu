@@ -1,10 +1,8 @@
 // gel.cu -- the gel lattice-spring model (FP64) and the marker exchange, sm_100a.
 //
-//   gel_kernel          one cluster of 8 CTAs (8 SMs) per gel; every phase of
-//                       Gel::stepElasticity, Gel::stepChemistry,
-//                       Gel::recordCenter and the gather of
-//                       Coupler::packFromGels, separated by cluster barriers
-//                       (gel_batch_kernel: one CTA per gel, block barriers).
+//   gel_kernel          one CTA per gel; every phase of Gel::stepElasticity,
+//                       Gel::stepChemistry, Gel::recordCenter and the gather of
+//                       Coupler::packFromGels, separated by block barriers.
 //   conc_markers_kernel one warp per marker: concentration sample, Robin flux,
 //                       delta-4 spread into the source field (Fluid::stepConcentration
 //                       marker part), optionally the un_robin scatter.
@@ -21,12 +19,9 @@
 //   k_gather_boundary src/coupling_kernels.cu:42   k_add_reaction_to_gel :8
 //   k_gel_repulsion :90   k_ibm_sample_concentration src/fluid_kernels.cu:350
 //   k_robin_boundary :293  k_ibm_spread_concentration :414
-#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include "gel.h"
-
-namespace cg = cooperative_groups;
 
 namespace glsm {
 
@@ -77,29 +72,12 @@ struct Idx {
     __device__ __forceinline__ int n(int x, int y, int z) const { return x + (LX + 2) * (y + (LY + 2) * z); }
 };
 
-// The threads that work on one gel: one CTA (the batched kernel), or a
-// thread-block cluster of kGelCluster CTAs on as many SMs (gel_kernel), whose
-// phases are separated by cluster barriers.  Release/acquire cluster
-// barriers order every phase's global-memory writes before the next phase's
-// reads by any thread of the cluster.
-struct Team {
-    int tid;       // thread index within the team
-    int n;         // threads of the team
-    bool cluster;  // the team is a cluster (else one CTA)
-    __device__ __forceinline__ void sync() const {
-        if (cluster)
-            cg::this_cluster().sync();
-        else
-            __syncthreads();
-    }
-};
-
-// loop over an inclusive 3-D index range with all threads of the team T
+// loop over an inclusive 3-D index range with all threads of the CTA
 #define GEL_FOR3(x0, x1, y0, y1, z0, z1, ...)                                           \
     {                                                                                   \
         const int _nx = (x1) - (x0) + 1, _ny = (y1) - (y0) + 1, _nz = (z1) - (z0) + 1;  \
         const int _cnt = _nx * _ny * _nz;                                               \
-        for (int _t = T.tid; _t < _cnt; _t += T.n) {                                    \
+        for (int _t = threadIdx.x; _t < _cnt; _t += blockDim.x) {                       \
             const int x = (x0) + _t % _nx;                                              \
             const int y = (y0) + (_t / _nx) % _ny;                                      \
             const int z = (z0) + _t / (_nx * _ny);                                      \
@@ -113,7 +91,7 @@ __device__ __forceinline__ int inward(int c, int top) { return c == 0 ? 1 : (c =
 // ---------------------------------------------------------------------------
 // mechanics phases (every 5th iteration)
 // ---------------------------------------------------------------------------
-__device__ void element_geometry(const GelDev& G, const Idx& I, const Team& T) {
+__device__ void element_geometry(const GelDev& G, const Idx& I) {
     GEL_FOR3(0, G.LX, 0, G.LY, 0, G.LZ, {
         const int e = I.e(x, y, z);
         double3 p[8];
@@ -176,7 +154,7 @@ _Pragma("unroll")
     })
 }
 
-__device__ void ghost_nodes(const GelDev& G, const Idx& I, const Team& T) {
+__device__ void ghost_nodes(const GelDev& G, const Idx& I) {
     GEL_FOR3(0, G.LX + 1, 0, G.LY + 1, 0, G.LZ + 1, {
         const int ox = inward(x, G.LX + 1), oy = inward(y, G.LY + 1), oz = inward(z, G.LZ + 1);
         if (ox | oy | oz) {
@@ -188,7 +166,7 @@ __device__ void ghost_nodes(const GelDev& G, const Idx& I, const Team& T) {
 }
 
 // no-flux ghost elements + normalised concentrations; and the osmotic pressure
-__device__ void chem_boundary_and_pressure(const GelDev& G, const Idx& I, const Team& T) {
+__device__ void chem_boundary_and_pressure(const GelDev& G, const Idx& I) {
     GEL_FOR3(0, G.LX, 0, G.LY, 0, G.LZ, {
         const int e = I.e(x, y, z);
         const int ox = inward(x, G.LX), oy = inward(y, G.LY), oz = inward(z, G.LZ);
@@ -214,7 +192,7 @@ __device__ void chem_boundary_and_pressure(const GelDev& G, const Idx& I, const 
     })
 }
 
-__device__ void node_averages(const GelDev& G, const Idx& I, const Team& T) {
+__device__ void node_averages(const GelDev& G, const Idx& I) {
     GEL_FOR3(1, G.LX, 1, G.LY, 1, G.LZ, {
         double su = 0, sv = 0;
 _Pragma("unroll")
@@ -230,7 +208,7 @@ _Pragma("unroll")
 }
 
 // nodal elastic + osmotic force, mobility, velocities; then setZero
-__device__ void node_forces(const GelDev& G, const Idx& I, const Team& T) {
+__device__ void node_forces(const GelDev& G, const Idx& I) {
     GEL_FOR3(1, G.LX, 1, G.LY, 1, G.LZ, {
         const int n = I.n(x, y, z);
         double wn = 0;
@@ -268,7 +246,7 @@ _Pragma("unroll")
 }
 
 // rn += dtx Veln (+ anchor of the bottom layer)
-__device__ void advance(const GelDev& G, const Idx& I, const Team& T) {
+__device__ void advance(const GelDev& G, const Idx& I) {
     GEL_FOR3(1, G.LX, 1, G.LY, 1, G.LZ, {
         const int n = I.n(x, y, z);
         double3 r = add(G.rn[n], mul(G.dtx, G.Veln[n]));
@@ -280,7 +258,7 @@ __device__ void advance(const GelDev& G, const Idx& I, const Team& T) {
     })
 }
 
-__device__ void terms(const GelDev& G, const Idx& I, const Team& T) {
+__device__ void terms(const GelDev& G, const Idx& I) {
     GEL_FOR3(1, G.LX - 1, 1, G.LY - 1, 1, G.LZ - 1, {
         const int e = I.e(x, y, z);
         const double w = G.wm[e], u = G.um_norm[e];
@@ -323,7 +301,7 @@ _Pragma("unroll")
 // ---------------------------------------------------------------------------
 // per-iteration phases
 // ---------------------------------------------------------------------------
-__device__ void set_zero(const GelDev& G, const Idx& I, const Team& T) {
+__device__ void set_zero(const GelDev& G, const Idx& I) {
     GEL_FOR3(1, G.LX, 1, G.LY, 1, G.LZ, {
         const int n = I.n(x, y, z);
         G.un_robin[n] = 0;
@@ -331,7 +309,7 @@ __device__ void set_zero(const GelDev& G, const Idx& I, const Team& T) {
     })
 }
 
-__device__ void chemistry(const GelDev& G, const Idx& I, const Team& T) {
+__device__ void chemistry(const GelDev& G, const Idx& I) {
     GEL_FOR3(1, G.LX - 1, 1, G.LY - 1, 1, G.LZ - 1, {
         const int e = I.e(x, y, z);
         if (void_element(G, y, z)) {
@@ -348,7 +326,7 @@ __device__ void chemistry(const GelDev& G, const Idx& I, const Team& T) {
 
 // Gel::fireExcitationPulse (src/gel.cu:751-783): u above threshold, v low on
 // the first tenth of the gel along x
-__device__ void fire_pulse(const GelDev& G, const Idx& I, const Team& T) {
+__device__ void fire_pulse(const GelDev& G, const Idx& I) {
     const int pw = max(1, G.LX / 10);
     GEL_FOR3(1, pw, 1, G.LY, 1, G.LZ, {
         if (!void_element(G, y, z)) {
@@ -359,8 +337,8 @@ __device__ void fire_pulse(const GelDev& G, const Idx& I, const Team& T) {
     })
 }
 
-__device__ void record_center(const GelDev& G, const Idx& I, int iter, const Team& T) {
-    if (T.tid != 0 || !G.series || G.series_every <= 0 || iter % G.series_every) return;
+__device__ void record_center(const GelDev& G, const Idx& I, int iter) {
+    if (threadIdx.x != 0 || !G.series || G.series_every <= 0 || iter % G.series_every) return;
     const int slot = (iter / G.series_every) % G.series_cap;
     double* r = G.series + 12 * (long long)slot;
     const int e = I.e(G.LX / 2, G.LY / 2, G.LZ / 2);
@@ -381,14 +359,11 @@ __device__ void record_center(const GelDev& G, const Idx& I, int iter, const Tea
 }
 
 // k_gather_boundary + the per-iteration stencil cache and the force-region box
-// (the box is reduced in the shared memory of the team's first CTA, which the
-// cluster's other CTAs reach as distributed shared memory)
-__device__ void gather(const GelDev& G, const GelArgs& a, int gel_index, int* s_box, const Team& T) {
+__device__ void gather(const GelDev& G, const GelArgs& a, int gel_index, int* s_box) {
     const MarkerDev& Mk = a.Mk;
-    int* box = T.cluster ? cg::this_cluster().map_shared_rank(s_box, 0) : s_box;
-    if (T.tid < 6) box[T.tid] = (T.tid & 1) ? -1 : 0x7fffffff;
-    T.sync();
-    for (int j = T.tid; j < G.M; j += T.n) {
+    if (threadIdx.x < 6) s_box[threadIdx.x] = (threadIdx.x & 1) ? -1 : 0x7fffffff;
+    __syncthreads();
+    for (int j = threadIdx.x; j < G.M; j += blockDim.x) {
         const int l = G.marker_off + j;
         const int id = G.bIndex[j];
         const double3 r = G.rn[id], v = G.Vels[id];
@@ -419,8 +394,8 @@ _Pragma("unroll")
                 }
             }
             if (hi >= 0) {
-                atomicMin(&box[2 * d], lo);
-                atomicMax(&box[2 * d + 1], hi);
+                atomicMin(&s_box[2 * d], lo);
+                atomicMax(&s_box[2 * d + 1], hi);
             }
         }
         float ws = 0.f;
@@ -436,72 +411,67 @@ _Pragma("unroll")
         Mk.wsum[l] = ws;
         if (ws == 0.f) atomicOr(&a.ctl->error, kErrMarkerOut);
     }
-    T.sync();
-    if (T.tid == 0) {
+    __syncthreads();
+    if (threadIdx.x == 0) {
         Box b;
-        b.x0 = box[0];
-        b.x1 = box[1];
-        b.y0 = box[2];
-        b.y1 = box[3];
-        b.z0 = box[4];
-        b.z1 = box[5];
+        b.x0 = s_box[0];
+        b.x1 = s_box[1];
+        b.y0 = s_box[2];
+        b.y1 = s_box[3];
+        b.z0 = s_box[4];
+        b.z1 = s_box[5];
         if (b.x1 < 0 || b.y1 < 0 || b.z1 < 0) b = Box{1, 0, 1, 0, 1, 0};
         Mk.boxes[gel_index] = b;
     }
 }
 
-// every phase of one gel, run by one team (a CTA or a cluster)
-__device__ void gel_run(const GelArgs& a, int gel_index, int* s_box, const Team& T) {
+// every phase of one gel, run by one CTA
+__device__ void gel_run(const GelArgs& a, int gel_index, int* s_box) {
     const GelDev& G = a.gels[gel_index];
     const Idx I{G.LX, G.LY};
     const int iter = a.iter_arg >= 0 ? a.iter_arg : a.ctl->iter;
     bool active = true;
     if ((a.phases & kPhAuto) && G.active_from > 0) {
         if (iter == G.active_from) {
-            fire_pulse(G, I, T);
-            T.sync();
+            fire_pulse(G, I);
+            __syncthreads();
         }
         active = iter >= G.active_from;
     }
     if ((a.phases & kPhElastic) && active) {
         if (iter % 5 == 0) {
-            ghost_nodes(G, I, T);
-            T.sync();
-            element_geometry(G, I, T);
-            T.sync();
-            chem_boundary_and_pressure(G, I, T);
-            T.sync();
-            node_averages(G, I, T);
-            T.sync();
-            node_forces(G, I, T);
-            T.sync();
-            advance(G, I, T);
-            T.sync();  // the anchor zeroes Veln before calTermsD reads it
-            terms(G, I, T);
-            T.sync();
+            ghost_nodes(G, I);
+            __syncthreads();
+            element_geometry(G, I);
+            __syncthreads();
+            chem_boundary_and_pressure(G, I);
+            __syncthreads();
+            node_averages(G, I);
+            __syncthreads();
+            node_forces(G, I);
+            __syncthreads();
+            advance(G, I);
+            __syncthreads();  // the anchor zeroes Veln before calTermsD reads it
+            terms(G, I);
+            __syncthreads();
         }
-        set_zero(G, I, T);
-        T.sync();
+        set_zero(G, I);
+        __syncthreads();
     }
     if ((a.phases & kPhChem) && active) {
-        chemistry(G, I, T);
-        T.sync();
+        chemistry(G, I);
+        __syncthreads();
     }
     if (a.phases & kPhRecord) {
-        record_center(G, I, iter, T);
-        T.sync();
+        record_center(G, I, iter);
+        __syncthreads();
     }
-    if (a.phases & kPhGather) gather(G, a, gel_index, s_box, T);
-    // no CTA of a cluster leaves while another may still reach its shared memory
-    if (T.cluster) T.sync();
+    if (a.phases & kPhGather) gather(G, a, gel_index, s_box);
 }
 
-// one cluster of kGelCluster CTAs per gel: cluster c runs gel c + first_gel
 __global__ void __launch_bounds__(kGelThreads) gel_kernel(GelArgs a) {
     __shared__ int s_box[6];
-    const cg::cluster_group cl = cg::this_cluster();
-    const Team T{(int)(cl.block_rank() * blockDim.x + threadIdx.x), (int)(cl.num_blocks() * blockDim.x), true};
-    gel_run(a, blockIdx.x / kGelCluster + a.first_gel, s_box, T);
+    gel_run(a, blockIdx.x + a.first_gel, s_box);
 }
 
 // batched: CTA b runs gel entries[b].first_gel of the system described by entries[b]
@@ -510,7 +480,7 @@ __global__ void __launch_bounds__(kGelThreads) gel_batch_kernel(const GelArgs* e
     if ((int)blockIdx.x >= n) return;
     const GelArgs& a = entries[blockIdx.x];
     if (a.dyn && a.dyn->remaining == 0) return;
-    gel_run(a, a.first_gel, s_box, Team{(int)threadIdx.x, (int)blockDim.x, false});
+    gel_run(a, a.first_gel, s_box);
 }
 
 // ---------------------------------------------------------------------------
@@ -678,18 +648,8 @@ __global__ void scatter_kernel(GelDev* gels, MarkerDev Mk) {
 // ---------------------------------------------------------------------------
 cudaError_t launch_gel(const GelArgs& a, int n_gels, cudaStream_t s) {
     if (n_gels <= 0) return cudaSuccess;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeClusterDimension;
-    attr[0].val.clusterDim.x = kGelCluster;
-    attr[0].val.clusterDim.y = 1;
-    attr[0].val.clusterDim.z = 1;
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(n_gels * kGelCluster));
-    cfg.blockDim = dim3(kGelThreads);
-    cfg.stream = s;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, gel_kernel, a);
+    gel_kernel<<<n_gels, kGelThreads, 0, s>>>(a);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_conc_markers(const MarkerArgs& a, cudaStream_t s) {

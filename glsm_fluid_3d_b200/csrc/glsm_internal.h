@@ -20,8 +20,7 @@ constexpr int kCellsPerThread = GLSM_LBM_CELLS_PER_THREAD;
 constexpr int kTileCells = kTile * kCellsPerThread;  // lattice cells per LBM ticket
 constexpr int kMarkersPerTask = kTile / 32;  // IBM task CTA: one warp per marker
 constexpr int kMaxBoxes = 64;     // force-region boxes (one per gel) seen by one LBM launch
-constexpr int kGelThreads = 512;  // threads of a CTA of the gel kernels
-constexpr int kGelCluster = 8;    // CTAs (on as many SMs) that work on one gel in gel_kernel
+constexpr int kGelThreads = 512;  // threads of the one-CTA-per-gel kernel
 
 enum Storage : int { kStoreF32 = 0, kStoreF16 = 1, kStoreBF16 = 2 };
 
