@@ -105,6 +105,7 @@ struct glsm_fluid_s {
     int lbm_ctas = 0;            // resident CTAs of the persistent substep kernel (odd substeps)
     int lbm_ctas_even = 0;       // the same for even substeps
     int wait_extra = 0;          // test aid (glsm_test_ibm_wait_extra): > 0 makes the IBM wait run out
+    long long dev_iter = -1;     // the device's iteration counter (Ctl::iter) after glsm_fluid_run; -1: unknown
     int device = 0;              // CUDA device the system lives on
     int l2_on = 0;              // keep the population array L2-persisting (glsm_fluid_set_l2_persisting)
     unsigned long long l2_bytes = 0;  // access-policy window of the substep launches (0: none)
@@ -1317,8 +1318,14 @@ int glsm_fluid_run(glsm_fluid f, int iter0, int n) {
     if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
     if (n == 0) return GLSM_OK;
     glsm_coupler c = f->c;
-    set_iter_kernel<<<1, 1, 0, c->stream>>>(c->d_ctl, iter0);
-    CK(cudaGetLastError());
+    // the graphs read the iteration from the control block and advance it; it
+    // is set only when it is not already iter0 (a run continuing the last one)
+    if (f->dev_iter != iter0) {
+        f->dev_iter = -1;
+        set_iter_kernel<<<1, 1, 0, c->stream>>>(c->d_ctl, iter0);
+        CK(cudaGetLastError());
+    }
+    f->dev_iter = -1;
     for (int it = 0; it < n; it++) {
         const int p0 = (int)(f->substeps & 1);
         cudaGraphExec_t ge;
@@ -1328,6 +1335,7 @@ int glsm_fluid_run(glsm_fluid f, int iter0, int n) {
         f->substeps += f->F.nsub;
         f->cur ^= 1;
     }
+    f->dev_iter = (long long)iter0 + n;
     return GLSM_OK;
 }
 
@@ -1847,6 +1855,7 @@ int glsm_batch_add(glsm_batch b, glsm_fluid f, int iter0, int n_iters) {
     if (b->sys.empty()) b->nsub = f->F.nsub;
     set_iter_kernel<<<1, 1, 0, b->stream>>>(f->c->d_ctl, iter0);
     CK(cudaGetLastError());
+    f->dev_iter = -1;  // the batch advances the counter
     f->batch = b;
     b->sys.push_back(f);
     b->remaining.push_back(n_iters > 0 ? n_iters : -1);
@@ -2097,6 +2106,7 @@ int glsm_checkpoint_load(glsm_fluid f, const void* buf, size_t bytes) {
     }
     f->cur = h.cur;
     f->substeps = h.substeps;
+    f->dev_iter = -1;  // the control block (iteration counter) came from the checkpoint
     return GLSM_OK;
 }
 
