@@ -75,6 +75,7 @@ struct glsm_gel_s {
     int index = -1;             // position in the coupler
     bool release_with_coupler = false;  // destroyed while coupled: freed with the coupler
     Snapshot snap;              // output snapshot (glsm_gel_snapshot)
+    bool ptr_out = false;       // a device pointer was handed out: the fused run gathers every iteration
 };
 
 struct glsm_coupler_s {
@@ -84,6 +85,8 @@ struct glsm_coupler_s {
     void* arena = nullptr;
     size_t bytes = 0;
     Ctl* d_ctl = nullptr;
+    int* d_fresh = nullptr;  // per gel: marker arrays current (kPhGatherStale)
+    bool markers_stale = true;  // host: a gel changed since the last fused run (fresh flags to clear)
     Ctl* h_ctl = nullptr;  // pinned mirror for error reads
     cudaStream_t stream = nullptr, side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -91,6 +94,11 @@ struct glsm_coupler_s {
     float rep_delta = 1e-4f, rep_gamma = 1.5f;  // src/coupling.cu:75-76
     glsm_fluid_s* fluid = nullptr;
 };
+
+// the fused run re-gathers the markers of a coupler whose gels changed
+static void mark_markers_stale(glsm_gel_s* g) {
+    if (g && g->coupler) g->coupler->markers_stale = true;
+}
 
 struct glsm_fluid_s {
     glsm_fluid_desc desc{};
@@ -147,7 +155,10 @@ static double noise_unit(uint64_t seed, uint64_t gel_id, uint64_t slot, uint64_t
 
 static cudaStream_t gel_stream(const glsm_gel_s* g) { return g->coupler ? g->coupler->stream : g->own; }
 
+static void mark_markers_stale(glsm_gel_s* g);
+
 static int upload_gel_desc(glsm_gel_s* g) {
+    mark_markers_stale(g);
     CK(cudaMemcpyAsync(g->d_self, &g->d, sizeof(GelDev), cudaMemcpyHostToDevice, gel_stream(g)));
     if (g->coupler)
         CK(cudaMemcpyAsync(g->coupler->d_gels + g->index, &g->d, sizeof(GelDev), cudaMemcpyHostToDevice,
@@ -424,6 +435,7 @@ static int gel_launch(glsm_gel g, int phases, int iter) {
     }
     a.phases = phases;
     a.iter_arg = iter;
+    mark_markers_stale(g);
     CK(launch_gel(a, 1, gel_stream(g)));
     return GLSM_OK;
 }
@@ -512,12 +524,17 @@ int glsm_gel_write(glsm_gel g, int field, const double* src, size_t count) {
     FieldRef f = gel_field(g, field);
     if (!f.ptr) return fail(GLSM_ERR_ARG, "unknown gel field %d", field);
     if (count != f.count) return fail(GLSM_ERR_ARG, "field %d holds %zu doubles", field, f.count);
+    mark_markers_stale(g);
     CK(cudaMemcpyAsync(f.ptr, src, f.count * sizeof(double), cudaMemcpyHostToDevice, gel_stream(g)));
     CK(cudaStreamSynchronize(gel_stream(g)));
     return GLSM_OK;
 }
 
-void* glsm_gel_device_ptr(glsm_gel g, int field) { return g ? gel_field(g, field).ptr : nullptr; }
+void* glsm_gel_device_ptr(glsm_gel g, int field) {
+    if (!g) return nullptr;
+    g->ptr_out = true;  // writes through it are invisible to the host
+    return gel_field(g, field).ptr;
+}
 
 int glsm_gel_filament(glsm_gel g, double* xyz, size_t max_points, size_t* n_points) {
     if (!g || !n_points || (max_points && !xyz)) return fail(GLSM_ERR_ARG, "null argument");
@@ -709,6 +726,7 @@ int glsm_coupler_create(const glsm_gel* gels, int n_gels, glsm_coupler* out) {
         cv.take<Box>(kMaxBoxes);
         cv.take<int2>(kMaxBoxes);
         cv.take<Ctl>(1);
+        cv.take<int>(kMaxBoxes);
         bytes = align_up(cv.off, 256);
     }
     cudaError_t e = cudaMalloc(&c->arena, bytes);
@@ -737,6 +755,7 @@ int glsm_coupler_create(const glsm_gel* gels, int n_gels, glsm_coupler* out) {
     mk.boxes = cv.take<Box>(kMaxBoxes);
     mk.gel_range = cv.take<int2>(kMaxBoxes);
     c->d_ctl = cv.take<Ctl>(1);
+    c->d_fresh = cv.take<int>(kMaxBoxes);
     std::vector<int> owner(M);
     int off = 0;
     for (int i = 0; i < n_gels; i++) {
@@ -1249,6 +1268,15 @@ int glsm_fluid_step_velocity(glsm_fluid f, int iter) {
     return GLSM_OK;
 }
 
+// the advection launch's arguments for concentration buffer cur
+static ConcArgs conc_args(glsm_fluid f, int cur, int bump_iter) {
+    glsm_coupler c = f->c;
+    ConcArgs a{f->F, c->mk, c->d_ctl, (int)c->gels.size(), cur, bump_iter, make_fastdiv((unsigned)f->F.nx),
+               make_fastdiv((unsigned)(f->F.nx * f->F.ny)), 0, 1};
+    conc_layout(a);
+    return a;
+}
+
 int glsm_fluid_step_concentration(glsm_fluid f, int iter) {
     if (!f || iter < 0) return fail(GLSM_ERR_ARG, "bad argument");
     if (f->batch) return fail(GLSM_ERR_STATE, "system is in a batch");
@@ -1256,9 +1284,7 @@ int glsm_fluid_step_concentration(glsm_fluid f, int iter) {
     MarkerArgs m{c->d_gels, c->mk, f->F.c[f->cur], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 0,
                  f->F.det_spread};
     CK(launch_conc_markers(m, c->stream));
-    ConcArgs a{f->F, c->mk, c->d_ctl, (int)c->gels.size(), f->cur, 0, make_fastdiv((unsigned)f->F.nx),
-               make_fastdiv((unsigned)(f->F.nx * f->F.ny))};
-    CK(launch_conv_diff(a, c->stream));
+    CK(launch_conv_diff(conc_args(f, f->cur, 0), c->stream));
     f->cur ^= 1;
     return GLSM_OK;
 }
@@ -1271,9 +1297,15 @@ static int enqueue_iteration(glsm_fluid f, int iter_arg, int p0, int cur) {
     glsm_coupler c = f->c;
     cudaStream_t s = c->stream;
     const int nsub = f->F.nsub;
-    CK(cudaMemsetAsync(f->d_sync, 0, 2 * sizeof(unsigned) * nsub, s));
-    const int phases = kPhElastic | kPhChem | kPhRecord | kPhGather | kPhAuto;
-    CK(launch_gel(coupler_gel_args(c, phases, iter_arg), (int)c->gels.size(), s));
+    // the gel kernel zeroes the substeps' ticket counters and gathers the
+    // markers only after the nodes moved (or first in a run call)
+    const int phases = kPhElastic | kPhChem | kPhRecord | kPhGather | kPhAuto | kPhGatherStale;
+    GelArgs ga = coupler_gel_args(c, phases, iter_arg);
+    ga.gather_fresh = c->d_fresh;
+    ga.zero_words = f->d_sync;
+    ga.n_zero_words = 2 * nsub;
+    if (c->gels.empty()) CK(cudaMemsetAsync(f->d_sync, 0, 2 * sizeof(unsigned) * nsub, s));
+    CK(launch_gel(ga, (int)c->gels.size(), s));
     // markers' concentration exchange and repulsion run beside the substeps
     CK(cudaEventRecord(c->ev_fork, s));
     CK(cudaStreamWaitEvent(c->side, c->ev_fork, 0));
@@ -1285,9 +1317,7 @@ static int enqueue_iteration(glsm_fluid f, int iter_arg, int p0, int cur) {
     CK(cudaEventRecord(c->ev_join, c->side));
     for (int k = 0; k < nsub; k++) CK(launch_substep(step_args(f, k, iter_arg), (p0 + k) & 1, s));
     CK(cudaStreamWaitEvent(s, c->ev_join, 0));
-    ConcArgs a{f->F, c->mk, c->d_ctl, (int)c->gels.size(), cur, iter_arg < 0 ? 1 : 0,
-               make_fastdiv((unsigned)f->F.nx), make_fastdiv((unsigned)(f->F.nx * f->F.ny))};
-    CK(launch_conv_diff(a, s));
+    CK(launch_conv_diff(conc_args(f, cur, iter_arg < 0 ? 1 : 0), s));
     return GLSM_OK;
 }
 
@@ -1324,6 +1354,15 @@ int glsm_fluid_run(glsm_fluid f, int iter0, int n) {
         f->dev_iter = -1;
         set_iter_kernel<<<1, 1, 0, c->stream>>>(c->d_ctl, iter0);
         CK(cudaGetLastError());
+    }
+    // the first iteration gathers the markers afresh when a gel changed since
+    // the last run (fields, parameters, per-method steps, checkpoints) or may
+    // have (a device pointer is out); otherwise the marker arrays are current
+    bool stale = c->markers_stale;
+    for (glsm_gel_s* g : c->gels) stale |= g->ptr_out;
+    if (stale) {
+        CK(cudaMemsetAsync(c->d_fresh, 0, sizeof(int) * c->gels.size(), c->stream));
+        c->markers_stale = false;
     }
     f->dev_iter = -1;
     for (int it = 0; it < n; it++) {
@@ -1674,8 +1713,7 @@ static int batch_rebuild(glsm_batch_s* b) {
         glsm_coupler c = f->c;
         StepArgs a = step_args(f, 0, -1, false);
         hs[i].step = a;
-        hs[i].conc = ConcArgs{f->F, c->mk, c->d_ctl, (int)c->gels.size(), 0, 0, make_fastdiv((unsigned)f->F.nx),
-                              make_fastdiv((unsigned)(f->F.nx * f->F.ny))};
+        hs[i].conc = conc_args(f, 0, 0);
         hd[i].parity0 = (int)(f->substeps & 1);
         hd[i].cur = f->cur;
         hd[i].remaining = (int)std::min<long long>(b->remaining[i], 1 << 30);
@@ -1689,7 +1727,7 @@ static int batch_rebuild(glsm_batch_s* b) {
             ga.first_gel = g;
             hg.push_back(ga);
         }
-        conv_off[i + 1] = conv_off[i] + (int)((f->F.N + kTile - 1) / kTile);
+        conv_off[i + 1] = conv_off[i] + conc_blocks(hs[i].conc);
         warp_off[i + 1] = warp_off[i] + c->mk.M;
         rep_off[i + 1] = rep_off[i] + c->mk.M;  // one warp per marker
     }
@@ -1870,6 +1908,7 @@ int glsm_batch_remove(glsm_batch b, glsm_fluid f) {
     b->sys.erase(b->sys.begin() + at);
     b->remaining.erase(b->remaining.begin() + at);
     f->batch = nullptr;
+    f->c->markers_stale = true;
     b->dirty = true;
     return GLSM_OK;
 }
@@ -2093,6 +2132,7 @@ int glsm_checkpoint_load(glsm_fluid f, const void* buf, size_t bytes) {
     CK(cudaMemcpy(f->arena, p, f->bytes, cudaMemcpyHostToDevice));
     p += f->bytes;
     CK(cudaMemcpy((char*)c->arena + coupler_plain_off(c), p, h.coupler_bytes, cudaMemcpyHostToDevice));
+    c->markers_stale = true;
     p += h.coupler_bytes;
     for (uint32_t i = 0; i < h.n_gels; i++) {
         glsm_gel_s* g = c->gels[i];

@@ -19,6 +19,7 @@
 //   k_gather_boundary src/coupling_kernels.cu:42   k_add_reaction_to_gel :8
 //   k_gel_repulsion :90   k_ibm_sample_concentration src/fluid_kernels.cu:350
 //   k_robin_boundary :293  k_ibm_spread_concentration :414
+#include <atomic>
 #include <cuda_runtime.h>
 
 #include "gel.h"
@@ -91,67 +92,121 @@ __device__ __forceinline__ int inward(int c, int top) { return c == 0 ? 1 : (c =
 // ---------------------------------------------------------------------------
 // mechanics phases (every 5th iteration)
 // ---------------------------------------------------------------------------
-__device__ void element_geometry(const GelDev& G, const Idx& I) {
-    GEL_FOR3(0, G.LX, 0, G.LY, 0, G.LZ, {
-        const int e = I.e(x, y, z);
-        double3 p[8];
-        double3 c = d3(0, 0, 0);
+// Element slots are processed in passes of blockDim.x (slot t = x + (LX+1)(y +
+// (LY+1) z) by thread t - t0).  A pass's rm_loc (8 double3 per element) and
+// nmSm (6 double3) are staged in shared memory at odd strides and written out
+// as the contiguous byte ranges they are, coalesced: thread-per-element
+// stores of 24- and 18-double records would scatter every warp store over
+// 32 cache lines.
+constexpr int kLocStride = 25;   // doubles per element in the rm_loc stage (24 used)
+constexpr int kFaceStride = 19;  // doubles per element in the nmSm stage (18 used)
+constexpr size_t kGelStageBytes = (size_t)kGelThreads * (kLocStride + kFaceStride) * sizeof(double);
+
+// rm_loc and nmSm as node_forces and terms read them: from the stage when the
+// gel's element slots fit one pass of element_geometry (which then leaves the
+// whole arrays there), else from global memory; the same doubles either way
+struct GeomStage {
+    const double* s;
+    bool on;
+    __device__ __forceinline__ double3 loc(const GelDev& G, int e, int m) const {
+        if (!on) return G.rm_loc[8 * e + m];
+        const double* p = s + kLocStride * e + 3 * m;
+        return d3(p[0], p[1], p[2]);
+    }
+    __device__ __forceinline__ double3 face(const GelDev& G, int e, int f) const {
+        if (!on) return G.nmSm[6 * e + f];
+        const double* p = s + kLocStride * kGelThreads + kFaceStride * e + 3 * f;
+        return d3(p[0], p[1], p[2]);
+    }
+};
+
+__device__ __forceinline__ GeomStage geom_stage(const GelDev& G, const double* stage) {
+    return GeomStage{stage, (G.LX + 1) * (G.LY + 1) * (G.LZ + 1) <= (int)blockDim.x && blockDim.x == kGelThreads};
+}
+
+__device__ void element_geometry(const GelDev& G, const Idx& I, double* stage) {
+    const int ex = G.LX + 1, ey = G.LY + 1;
+    const int cnt = ex * ey * (G.LZ + 1);
+    for (int t0 = 0; t0 < cnt; t0 += blockDim.x) {
+        const int t = t0 + (int)threadIdx.x, n_pass = min((int)blockDim.x, cnt - t0);
+        double* st_loc = stage + kLocStride * threadIdx.x;
+        double* st_face = stage + kLocStride * blockDim.x + kFaceStride * threadIdx.x;
+        if (t < cnt) {
+            double3 p[8];
+            const int x = t % ex, y = (t / ex) % ey, z = t / (ex * ey);
+            const int e = I.e(x, y, z);
+            double3 c = d3(0, 0, 0);
 _Pragma("unroll")
-        for (int m = 0; m < 8; m++) {
-            p[m] = G.rn[I.n(x + (m >> 2), y + ((m >> 1) & 1), z + (m & 1))];
-            c = add(c, p[m]);
-        }
-        c = mul(1.0 / 8.0, c);
-        G.rm[e] = c;
+            for (int m = 0; m < 8; m++) {
+                p[m] = G.rn[I.n(x + (m >> 2), y + ((m >> 1) & 1), z + (m & 1))];
+                c = add(c, p[m]);
+            }
+            c = mul(1.0 / 8.0, c);
+            G.rm[e] = c;
 _Pragma("unroll")
-        for (int m = 0; m < 8; m++) {
-            p[m] = sub(p[m], c);
-            G.rm_loc[8 * e + m] = p[m];
-        }
-        // Outward face area vectors.  The reference integrates cross(dx/da, dx/db)
-        // of the bilinear face over 2x2 points at +-0.5 (src/gel_kernels.cu:255-436);
-        // for a bilinear face that sum equals (1/4) (sum_m a_m P_m) x (sum_m b_m P_m).
-        // corner m = 4i + 2j + k
-        const double3 ax0 = sub(add(p[2], p[3]), add(p[0], p[1])), bx0 = sub(add(p[1], p[3]), add(p[0], p[2]));
-        const double3 ax1 = sub(add(p[6], p[7]), add(p[4], p[5])), bx1 = sub(add(p[5], p[7]), add(p[4], p[6]));
-        const double3 ay0 = sub(add(p[4], p[5]), add(p[0], p[1])), by0 = sub(add(p[1], p[5]), add(p[0], p[4]));
-        const double3 ay1 = sub(add(p[6], p[7]), add(p[2], p[3])), by1 = sub(add(p[3], p[7]), add(p[2], p[6]));
-        const double3 az0 = sub(add(p[4], p[6]), add(p[0], p[2])), bz0 = sub(add(p[2], p[6]), add(p[0], p[4]));
-        const double3 az1 = sub(add(p[5], p[7]), add(p[1], p[3])), bz1 = sub(add(p[3], p[7]), add(p[1], p[5]));
-        G.nmSm[6 * e + 0] = mul(-0.25, crs(ax0, bx0));
-        G.nmSm[6 * e + 1] = mul(0.25, crs(ax1, bx1));
-        G.nmSm[6 * e + 2] = mul(0.25, crs(ay0, by0));
-        G.nmSm[6 * e + 3] = mul(-0.25, crs(ay1, by1));
-        G.nmSm[6 * e + 4] = mul(-0.25, crs(az0, bz0));
-        G.nmSm[6 * e + 5] = mul(0.25, crs(az1, bz1));
-        // Volume: det J of the trilinear map summed over the 2x2x2 points
-        // (+-0.5)^3 with unit weights (src/gel_kernels.cu:437-479).  With
-        // x = a0 + a1 s + a2 n + a3 t + a4 sn + a5 st + a6 nt + a7 snt:
-        double3 a1 = d3(0, 0, 0), a2 = a1, a3 = a1, a4 = a1, a5 = a1, a6 = a1, a7 = a1;
+            for (int m = 0; m < 8; m++) {
+                p[m] = sub(p[m], c);
+                st_loc[3 * m] = p[m].x;
+                st_loc[3 * m + 1] = p[m].y;
+                st_loc[3 * m + 2] = p[m].z;
+            }
+            // Outward face area vectors.  The reference integrates cross(dx/da, dx/db)
+            // of the bilinear face over 2x2 points at +-0.5 (src/gel_kernels.cu:255-436);
+            // for a bilinear face that sum equals (1/4) (sum_m a_m P_m) x (sum_m b_m P_m).
+            // corner m = 4i + 2j + k
+            const double3 ax0 = sub(add(p[2], p[3]), add(p[0], p[1])), bx0 = sub(add(p[1], p[3]), add(p[0], p[2]));
+            const double3 ax1 = sub(add(p[6], p[7]), add(p[4], p[5])), bx1 = sub(add(p[5], p[7]), add(p[4], p[6]));
+            const double3 ay0 = sub(add(p[4], p[5]), add(p[0], p[1])), by0 = sub(add(p[1], p[5]), add(p[0], p[4]));
+            const double3 ay1 = sub(add(p[6], p[7]), add(p[2], p[3])), by1 = sub(add(p[3], p[7]), add(p[2], p[6]));
+            const double3 az0 = sub(add(p[4], p[6]), add(p[0], p[2])), bz0 = sub(add(p[2], p[6]), add(p[0], p[4]));
+            const double3 az1 = sub(add(p[5], p[7]), add(p[1], p[3])), bz1 = sub(add(p[3], p[7]), add(p[1], p[5]));
+            const double3 face[6] = {mul(-0.25, crs(ax0, bx0)), mul(0.25, crs(ax1, bx1)), mul(0.25, crs(ay0, by0)),
+                                     mul(-0.25, crs(ay1, by1)), mul(-0.25, crs(az0, bz0)), mul(0.25, crs(az1, bz1))};
 _Pragma("unroll")
-        for (int m = 0; m < 8; m++) {
-            const double s = (m >> 2) ? 1.0 : -1.0, n = ((m >> 1) & 1) ? 1.0 : -1.0, t = (m & 1) ? 1.0 : -1.0;
-            a1 = add(a1, mul(s, p[m]));
-            a2 = add(a2, mul(n, p[m]));
-            a3 = add(a3, mul(t, p[m]));
-            a4 = add(a4, mul(s * n, p[m]));
-            a5 = add(a5, mul(s * t, p[m]));
-            a6 = add(a6, mul(n * t, p[m]));
-            a7 = add(a7, mul(s * n * t, p[m]));
-        }
-        double vol = 0;
+            for (int f = 0; f < 6; f++) {
+                st_face[3 * f] = face[f].x;
+                st_face[3 * f + 1] = face[f].y;
+                st_face[3 * f + 2] = face[f].z;
+            }
+            // Volume: det J of the trilinear map summed over the 2x2x2 points
+            // (+-0.5)^3 with unit weights (src/gel_kernels.cu:437-479).  With
+            // x = (a0 + a1 s + a2 n + a3 t + a4 sn + a5 st + a6 nt + a7 snt) / 8,
+            // where a_k is the sum of the corners signed by the corner's s, n, t
+            // factors (a butterfly over the three index bits), J's columns are
+            //   js = (a1 + n a4 + t a5 + nt a7) / 8, jn = (a2 + s a4 + t a6 + st a7) / 8,
+            //   jt = (a3 + s a5 + n a6 + sn a7) / 8,
+            // and the sum over s, n, t = +-h keeps only the terms even in each:
+            //   sum det J = (8 / 512) [a1.(a2 x a3) + h^2 (a1.(a4 x a5) + a4.(a2 x a6) + a5.(a6 x a3))].
+            double3 q[8];
 _Pragma("unroll")
-        for (int m = 0; m < 8; m++) {
-            const double s = (m >> 2) ? 0.5 : -0.5, n = ((m >> 1) & 1) ? 0.5 : -0.5, t = (m & 1) ? 0.5 : -0.5;
-            const double3 js = mul(0.125, add(add(a1, mul(n, a4)), add(mul(t, a5), mul(n * t, a7))));
-            const double3 jn = mul(0.125, add(add(a2, mul(s, a4)), add(mul(t, a6), mul(s * t, a7))));
-            const double3 jt = mul(0.125, add(add(a3, mul(s, a5)), add(mul(n, a6), mul(s * n, a7))));
-            vol += dot(js, crs(jn, jt));
+            for (int m = 0; m < 8; m++) q[m] = p[m];
+_Pragma("unroll")
+            for (int bit = 1; bit < 8; bit <<= 1) {
+_Pragma("unroll")
+                for (int m = 0; m < 8; m++) {
+                    if (m & bit) continue;
+                    const double3 lo = q[m], hi = q[m | bit];
+                    q[m] = add(lo, hi);
+                    q[m | bit] = sub(hi, lo);
+                }
+            }
+            // q[4] = a1 (s), q[2] = a2 (n), q[1] = a3 (t), q[6] = a4 (sn), q[5] = a5 (st), q[3] = a6 (nt)
+            const double3 a1 = q[4], a2 = q[2], a3 = q[1], a4 = q[6], a5 = q[5], a6 = q[3];
+            const double vol = (8.0 / 512.0) * (dot(a1, crs(a2, a3)) + 0.25 * (dot(a1, crs(a4, a5)) +
+                                                                                dot(a4, crs(a2, a6)) +
+                                                                                dot(a5, crs(a6, a3))));
+            G.vol[e] = vol;
+            G.wmp[e] = G.wm[e];
+            G.wm[e] = G.dx * G.dy * G.dz * G.FA0 / vol;
         }
-        G.vol[e] = vol;
-        G.wmp[e] = G.wm[e];
-        G.wm[e] = G.dx * G.dy * G.dz * G.FA0 / vol;
-    })
+        __syncthreads();
+        double* rl = reinterpret_cast<double*>(G.rm_loc + 8 * (size_t)t0);
+        for (int k = threadIdx.x; k < 24 * n_pass; k += blockDim.x) rl[k] = stage[kLocStride * (k / 24) + k % 24];
+        const double* sf = stage + kLocStride * blockDim.x;
+        double* nf = reinterpret_cast<double*>(G.nmSm + 6 * (size_t)t0);
+        for (int k = threadIdx.x; k < 18 * n_pass; k += blockDim.x) nf[k] = sf[kFaceStride * (k / 18) + k % 18];
+        __syncthreads();
+    }
 }
 
 __device__ void ghost_nodes(const GelDev& G, const Idx& I) {
@@ -208,7 +263,7 @@ _Pragma("unroll")
 }
 
 // nodal elastic + osmotic force, mobility, velocities; then setZero
-__device__ void node_forces(const GelDev& G, const Idx& I) {
+__device__ void node_forces(const GelDev& G, const Idx& I, const GeomStage& gs) {
     GEL_FOR3(1, G.LX, 1, G.LY, 1, G.LZ, {
         const int n = I.n(x, y, z);
         double wn = 0;
@@ -231,8 +286,8 @@ _Pragma("unroll")
             f1 = add(f1, sub(s, mul(4.0, r0)));
             // osmotic term: pressure times the element's faces that meet at the node
             const int e = I.e(a > 0 ? x : x - 1, b > 0 ? y : y - 1, c > 0 ? z : z - 1);
-            const double3 nf = add(add(G.nmSm[6 * e + (a > 0 ? 0 : 1)], G.nmSm[6 * e + (b > 0 ? 2 : 3)]),
-                                   G.nmSm[6 * e + (c > 0 ? 4 : 5)]);
+            const double3 nf = add(add(gs.face(G, e, a > 0 ? 0 : 1), gs.face(G, e, b > 0 ? 2 : 3)),
+                                   gs.face(G, e, c > 0 ? 4 : 5));
             f2 = add(f2, mul(G.pm[e], nf));
         }
         // the reference multiplies by pow(dx*dy*dz, 1/3) with an integer 1/3, i.e. by 1
@@ -258,7 +313,7 @@ __device__ void advance(const GelDev& G, const Idx& I) {
     })
 }
 
-__device__ void terms(const GelDev& G, const Idx& I) {
+__device__ void terms(const GelDev& G, const Idx& I, const GeomStage& gs) {
     GEL_FOR3(1, G.LX - 1, 1, G.LY - 1, 1, G.LZ - 1, {
         const int e = I.e(x, y, z);
         const double w = G.wm[e], u = G.um_norm[e];
@@ -270,14 +325,14 @@ __device__ void terms(const GelDev& G, const Idx& I) {
 _Pragma("unroll")
         for (int m = 0; m < 8; m++) {
             const int i = m >> 2, j = (m >> 1) & 1, k = m & 1;
-            const double3 rl = G.rm_loc[8 * e + m];
+            const double3 rl = gs.loc(G, e, m);
             const double N = 0.125 * (1 + (2 * i - 1) * rl.x) * (1 + (2 * j - 1) * rl.y) * (1 + (2 * k - 1) * rl.z);
             const int nn = I.n(x + i, y + j, z + k);
             vu = add(vu, mul(N * G.un_norm[nn], G.Veln[nn]));
         }
         double t1 = 0;
 _Pragma("unroll")
-        for (int f = 0; f < 6; f++) t1 += dot(G.nmSm[6 * e + f], vu);
+        for (int f = 0; f < 6; f++) t1 += dot(gs.face(G, e, f), vu);
         G.T1[e] = t1 / G.vol[e];
         // T2: -grad w . grad u + (1 - w) lap u with three-point derivatives on
         // the deformed (non-uniform) element-centre grid
@@ -377,6 +432,8 @@ __device__ void gather(const GelDev& G, const GelArgs& a, int gel_index, int* s_
         const int n[3] = {a.nx, a.ny, a.nz};
         int b0[3], valid = 0;
         float ph[3][4];
+        const unsigned act = __activemask();
+        const bool leader = (threadIdx.x & 31) == __ffs(act) - 1;
 _Pragma("unroll")
         for (int d = 0; d < 3; d++) {
             const int ic = (int)floorf(g[d]);
@@ -393,7 +450,10 @@ _Pragma("unroll")
                     hi = max(hi, cc);
                 }
             }
-            if (hi >= 0) {
+            // the warp's extent first, then one shared atomic per warp
+            lo = __reduce_min_sync(act, lo);
+            hi = __reduce_max_sync(act, hi);
+            if (leader && hi >= 0) {
                 atomicMin(&s_box[2 * d], lo);
                 atomicMax(&s_box[2 * d + 1], hi);
             }
@@ -426,11 +486,11 @@ _Pragma("unroll")
 }
 
 // every phase of one gel, run by one CTA
-__device__ void gel_run(const GelArgs& a, int gel_index, int* s_box) {
+__device__ void gel_run(const GelArgs& a, int gel_index, int* s_box, double* stage) {
     const GelDev& G = a.gels[gel_index];
     const Idx I{G.LX, G.LY};
     const int iter = a.iter_arg >= 0 ? a.iter_arg : a.ctl->iter;
-    bool active = true;
+    bool active = true, moved = false;
     if ((a.phases & kPhAuto) && G.active_from > 0) {
         if (iter == G.active_from) {
             fire_pulse(G, I);
@@ -440,19 +500,19 @@ __device__ void gel_run(const GelArgs& a, int gel_index, int* s_box) {
     }
     if ((a.phases & kPhElastic) && active) {
         if (iter % 5 == 0) {
+            moved = true;
             ghost_nodes(G, I);
             __syncthreads();
-            element_geometry(G, I);
-            __syncthreads();
+            element_geometry(G, I, stage);
             chem_boundary_and_pressure(G, I);
             __syncthreads();
             node_averages(G, I);
             __syncthreads();
-            node_forces(G, I);
+            node_forces(G, I, geom_stage(G, stage));
             __syncthreads();
             advance(G, I);
             __syncthreads();  // the anchor zeroes Veln before calTermsD reads it
-            terms(G, I);
+            terms(G, I, geom_stage(G, stage));
             __syncthreads();
         }
         set_zero(G, I);
@@ -466,12 +526,22 @@ __device__ void gel_run(const GelArgs& a, int gel_index, int* s_box) {
         record_center(G, I, iter);
         __syncthreads();
     }
-    if (a.phases & kPhGather) gather(G, a, gel_index, s_box);
+    if (a.phases & kPhGather) {
+        if (!(a.phases & kPhGatherStale)) {
+            gather(G, a, gel_index, s_box);
+        } else if (moved || !a.gather_fresh[gel_index]) {
+            gather(G, a, gel_index, s_box);  // every thread read the flag before its barriers
+            if (threadIdx.x == 0) a.gather_fresh[gel_index] = 1;
+        }
+    }
 }
 
 __global__ void __launch_bounds__(kGelThreads) gel_kernel(GelArgs a) {
     __shared__ int s_box[6];
-    gel_run(a, blockIdx.x + a.first_gel, s_box);
+    extern __shared__ double stage[];  // kGelStageBytes
+    if (blockIdx.x == 0)
+        for (int i = threadIdx.x; i < a.n_zero_words; i += blockDim.x) a.zero_words[i] = 0u;
+    gel_run(a, blockIdx.x + a.first_gel, s_box, stage);
 }
 
 // batched: CTA b runs gel entries[b].first_gel of the system described by entries[b]
@@ -480,7 +550,8 @@ __global__ void __launch_bounds__(kGelThreads) gel_batch_kernel(const GelArgs* e
     if ((int)blockIdx.x >= n) return;
     const GelArgs& a = entries[blockIdx.x];
     if (a.dyn && a.dyn->remaining == 0) return;
-    gel_run(a, a.first_gel, s_box);
+    extern __shared__ double stage[];  // kGelStageBytes
+    gel_run(a, a.first_gel, s_box, stage);
 }
 
 // ---------------------------------------------------------------------------
@@ -646,9 +717,27 @@ __global__ void scatter_kernel(GelDev* gels, MarkerDev Mk) {
 }
 
 // ---------------------------------------------------------------------------
+// the gel kernels' stage exceeds the default 48 KB of dynamic shared memory:
+// raise their limit once per device
+static cudaError_t gel_smem_limit() {
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const unsigned long long bit = 1ull << (dev & 63);
+    if (done.load() & bit) return cudaSuccess;
+    e = cudaFuncSetAttribute(gel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGelStageBytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(gel_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGelStageBytes);
+    if (e == cudaSuccess) done.fetch_or(bit);
+    return e;
+}
+
 cudaError_t launch_gel(const GelArgs& a, int n_gels, cudaStream_t s) {
     if (n_gels <= 0) return cudaSuccess;
-    gel_kernel<<<n_gels, kGelThreads, 0, s>>>(a);
+    cudaError_t e = gel_smem_limit();
+    if (e != cudaSuccess) return e;
+    gel_kernel<<<n_gels, kGelThreads, kGelStageBytes, s>>>(a);
     return cudaGetLastError();
 }
 
@@ -666,7 +755,9 @@ cudaError_t launch_repulsion(const RepulsionArgs& a, cudaStream_t s) {
 
 cudaError_t launch_gel_batch(const GelArgs* entries, int n, int grid, cudaStream_t s) {
     if (grid <= 0) return cudaSuccess;
-    gel_batch_kernel<<<grid, kGelThreads, 0, s>>>(entries, n);
+    cudaError_t e = gel_smem_limit();
+    if (e != cudaSuccess) return e;
+    gel_batch_kernel<<<grid, kGelThreads, kGelStageBytes, s>>>(entries, n);
     return cudaGetLastError();
 }
 

@@ -11,6 +11,9 @@ enum : int {
     kPhGather = 4,    // Coupler::packFromGels for this gel + stencil cache + box
     kPhRecord = 8,    // Gel::recordCenter (time series)
     kPhAuto = 16,     // honour active_from: skip before it, fire the pulse at it
+    kPhGatherStale = 32,  // with kPhGather: only when the mechanics moved the nodes in
+                          // this launch or gather_fresh[gel] is 0 (the marker arrays are
+                          // a function of the nodes, which nothing else changes in a run)
 };
 
 struct GelArgs {
@@ -24,6 +27,9 @@ struct GelArgs {
     float h;
     float g2l;         // gel -> lattice velocity factor
     const SysDyn* dyn; // batched systems: skip the gel when dyn->remaining == 0
+    int* gather_fresh; // kPhGatherStale: per gel, 1 while its marker arrays are current
+    unsigned* zero_words;  // zeroed by the first CTA before any phase (the substeps'
+    int n_zero_words;      // ticket counters of the iteration), or null
 };
 
 struct MarkerArgs {

@@ -13,6 +13,7 @@
 //   k_macros / k_collide          src/fluid_kernels.cu:98-111, :125-142
 //   k_stream_bounce               src/fluid_kernels.cu:144-165
 //   k_convection_diffusion        src/fluid_kernels.cu:177-242
+#include <algorithm>
 #include <cuda_bf16.h>
 #include <cstdlib>
 #include <cuda_fp16.h>
@@ -1056,64 +1057,76 @@ BatchKernel batch_kernel(int storage, int parity, int perx, int det, int f16_rou
 // ---------------------------------------------------------------------------
 // upwind advection + diffusion of the concentration (once per iteration)
 // ---------------------------------------------------------------------------
-// one 256-cell tile of the upwind advection + diffusion
+// One CTA: kTile consecutive cells of an xy plane (x fastest), each thread
+// marching its column through a.zc planes from z0 = bz * a.zc.  The column's
+// x and y neighbours are fixed, and the z neighbours' concentration and
+// vertical velocity pass from one plane to the next in registers, so a cell
+// costs five concentration and five velocity loads (the centre as one
+// float4).  The arithmetic is k_convection_diffusion's, term for term.
 template <bool DET>
-__device__ void conv_diff_tile(const ConcArgs& a, unsigned block, Box* s_b, int* s_g, int* s_nb_p) {
-    if (threadIdx.x == 0 && a.bump_iter && block == 0) a.ctl->iter += 1;  // nothing in this kernel reads it
+__device__ void conv_diff_cols(const ConcArgs& a, unsigned bx, unsigned bz, Box* s_b, int* s_g, int* s_nb_p) {
+    if (threadIdx.x == 0 && a.bump_iter && bx == 0 && bz == 0) a.ctl->iter += 1;  // nothing in this kernel reads it
     const FluidDev& F = a.F;
-    const unsigned nx = F.nx, ny = F.ny, nz = F.nz;
-    const unsigned N = (unsigned)F.N, nxy = nx * ny;
-    const unsigned c0 = block * kTile;
-    const unsigned c1 = min(c0 + kTile - 1, N - 1);
-    const TileExt ext = tile_extent(c0, c1, nx, ny, a.div_nx, a.div_nxy);
+    const unsigned nx = F.nx, ny = F.ny, nz = F.nz, nxy = nx * ny;
+    const unsigned p0 = bx * kTile, p1 = min(p0 + kTile - 1, nxy - 1);
+    const unsigned z0 = bz * (unsigned)a.zc, z1 = min(z0 + (unsigned)a.zc - 1, nz - 1);
+    TileExt ext = tile_extent(p0, p1, nx, ny, a.div_nx, a.div_nxy);  // one plane: z0 = z1 = 0
+    ext.z0 = (int)z0;
+    ext.z1 = (int)z1;
     const int nb = tile_boxes(a.Mk.boxes, a.n_boxes, ext, s_b, s_g, s_nb_p);
-    const unsigned i = c0 + threadIdx.x;
-    if (i > c1) return;
-    const unsigned z = fdiv(i, a.div_nxy);
-    const unsigned rem = i - z * nxy;
-    const unsigned y = fdiv(rem, a.div_nx);
-    const unsigned x = rem - y * nx;
-    bool inb = false;
-    for (int j = 0; j < nb; j++) inb |= inside(s_b[j], (int)x, (int)y, (int)z);
-
+    const unsigned p = p0 + threadIdx.x;
+    if (p > p1) return;
+    const unsigned y = fdiv(p, a.div_nx);
+    const unsigned x = p - y * nx;
     const unsigned xp = (x + 1 < nx) ? x + 1 : (F.per[0] ? 0 : x);
     const unsigned xm = (x >= 1) ? x - 1 : (F.per[0] ? nx - 1 : x);
     const unsigned yp = (y + 1 < ny) ? y + 1 : (F.per[1] ? 0 : y);
     const unsigned ym = (y >= 1) ? y - 1 : (F.per[1] ? ny - 1 : y);
-    const unsigned zp = (z + 1 < nz) ? z + 1 : (F.per[2] ? 0 : z);
-    const unsigned zm = (z >= 1) ? z - 1 : (F.per[2] ? nz - 1 : z);
-    const unsigned base = z * nxy + y * nx;
-    const unsigned ixp = base + xp, ixm = base + xm;
-    const unsigned iyp = z * nxy + yp * nx + x, iym = z * nxy + ym * nx + x;
-    const unsigned izp = zp * nxy + y * nx + x, izm = zm * nxy + y * nx + x;
+    const unsigned pxp = y * nx + xp, pxm = y * nx + xm, pyp = yp * nx + x, pym = ym * nx + x;
 
     const float* c1p = F.c[a.cur];
     float* c2p = F.c[a.cur ^ 1];
     const float* U = reinterpret_cast<const float*>(F.u);
-    const float c = c1p[i], cxp = c1p[ixp], cxm = c1p[ixm], cyp = c1p[iyp], cym = c1p[iym], czp = c1p[izp],
-                czm = c1p[izm];
-    const float ux = U[4 * i], uy = U[4 * i + 1], uz = U[4 * i + 2];
-    const float uL = 0.5f * (U[4 * ixm] + ux), uR = 0.5f * (ux + U[4 * ixp]);
-    const float vL = 0.5f * (U[4 * iym + 1] + uy), vR = 0.5f * (uy + U[4 * iyp + 1]);
-    const float wL = 0.5f * (U[4 * izm + 2] + uz), wR = 0.5f * (uz + U[4 * izp + 2]);
-    const float cLx = (uL >= 0.0f) ? cxm : c, cLy = (vL >= 0.0f) ? cym : c, cLz = (wL >= 0.0f) ? czm : c;
-    const float cRx = (uR >= 0.0f) ? c : cxp, cRy = (vR >= 0.0f) ? c : cyp, cRz = (wR >= 0.0f) ? c : czp;
     const float ih = F.inv_dx, ih2 = ih * ih;
-    const float conv = -((uR * cRx - uL * cLx) * ih + (vR * cRy - vL * cLy) * ih + (wR * cRz - wL * cLz) * ih);
-    const float diff = F.Dc * ((cxm - 2.0f * c + cxp) * ih2 + (cym - 2.0f * c + cyp) * ih2 + (czm - 2.0f * c + czp) * ih2);
-    float src = 0.f;
-    if (DET && inb) {
-        // deterministic spreads: the markers' concentration source, gathered
-        float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
-        const float inv_h3 = 1.0f / (F.h * F.h * F.h);
-        for (int j = 0; j < nb; j++)
-            if (inside(s_b[j], (int)x, (int)y, (int)z)) det_gather<true>(a.Mk, s_g[j], (int)x, (int)y, (int)z, inv_h3, acc);
-        src = acc.x;
-    } else if (inb) {
-        src = __ldcg(&F.source[i]);
-        __stcg(&F.source[i], 0.f);
+    const unsigned zm0 = (z0 >= 1) ? z0 - 1 : (F.per[2] ? nz - 1 : z0);
+    float czm = c1p[zm0 * nxy + p], uzm = U[4 * (zm0 * nxy + p) + 2];
+    float c = c1p[z0 * nxy + p];
+    float4 u = F.u[z0 * nxy + p];
+    for (unsigned z = z0; z <= z1; z++) {
+        const unsigned zp = (z + 1 < nz) ? z + 1 : (F.per[2] ? 0 : z);
+        const unsigned b = z * nxy, i = b + p;
+        const float czp = c1p[zp * nxy + p];
+        const float4 up = F.u[zp * nxy + p];
+        const float cxp = c1p[b + pxp], cxm = c1p[b + pxm], cyp = c1p[b + pyp], cym = c1p[b + pym];
+        const float ux = u.x, uy = u.y, uz = u.z;
+        const float uL = 0.5f * (U[4 * (b + pxm)] + ux), uR = 0.5f * (ux + U[4 * (b + pxp)]);
+        const float vL = 0.5f * (U[4 * (b + pym) + 1] + uy), vR = 0.5f * (uy + U[4 * (b + pyp) + 1]);
+        const float wL = 0.5f * (uzm + uz), wR = 0.5f * (uz + up.z);
+        const float cLx = (uL >= 0.0f) ? cxm : c, cLy = (vL >= 0.0f) ? cym : c, cLz = (wL >= 0.0f) ? czm : c;
+        const float cRx = (uR >= 0.0f) ? c : cxp, cRy = (vR >= 0.0f) ? c : cyp, cRz = (wR >= 0.0f) ? c : czp;
+        const float conv = -((uR * cRx - uL * cLx) * ih + (vR * cRy - vL * cLy) * ih + (wR * cRz - wL * cLz) * ih);
+        const float diff =
+            F.Dc * ((cxm - 2.0f * c + cxp) * ih2 + (cym - 2.0f * c + cyp) * ih2 + (czm - 2.0f * c + czp) * ih2);
+        bool inb = false;
+        for (int j = 0; j < nb; j++) inb |= inside(s_b[j], (int)x, (int)y, (int)z);
+        float src = 0.f;
+        if (DET && inb) {
+            // deterministic spreads: the markers' concentration source, gathered
+            float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+            const float inv_h3 = 1.0f / (F.h * F.h * F.h);
+            for (int j = 0; j < nb; j++)
+                if (inside(s_b[j], (int)x, (int)y, (int)z)) det_gather<true>(a.Mk, s_g[j], (int)x, (int)y, (int)z, inv_h3, acc);
+            src = acc.x;
+        } else if (inb) {
+            src = __ldcg(&F.source[i]);
+            __stcg(&F.source[i], 0.f);
+        }
+        c2p[i] = c + F.dtc * (conv + diff + src);
+        czm = c;
+        uzm = uz;
+        c = czp;
+        u = up;
     }
-    c2p[i] = c + F.dtc * (conv + diff + src);
 }
 
 template <bool DET>
@@ -1121,7 +1134,7 @@ __global__ void __launch_bounds__(kTile) conv_diff_kernel(ConcArgs a) {
     __shared__ int s_nb;
     __shared__ Box s_b[kMaxBoxes];
     __shared__ int s_g[kMaxBoxes];
-    conv_diff_tile<DET>(a, blockIdx.x, s_b, s_g, &s_nb);
+    conv_diff_cols<DET>(a, blockIdx.x, blockIdx.y, s_b, s_g, &s_nb);
 }
 
 __device__ __forceinline__ int find_system(const int* offsets, int n, unsigned t) {
@@ -1145,10 +1158,11 @@ __global__ void __launch_bounds__(kTile) conv_diff_batch_kernel(const BatchSys* 
     if (sys[s].dyn->remaining == 0) return;
     ConcArgs a = sys[s].conc;
     a.cur = sys[s].dyn->cur;
+    const unsigned lb = b - block_offsets[s];
     if (a.F.det_spread)
-        conv_diff_tile<true>(a, b - block_offsets[s], s_b, s_g, &s_nb);
+        conv_diff_cols<true>(a, lb % a.plane_blocks, lb / a.plane_blocks, s_b, s_g, &s_nb);
     else
-        conv_diff_tile<false>(a, b - block_offsets[s], s_b, s_g, &s_nb);
+        conv_diff_cols<false>(a, lb % a.plane_blocks, lb / a.plane_blocks, s_b, s_g, &s_nb);
 }
 
 // end of a batch iteration: advance every system's iteration, AA parity and
@@ -1405,8 +1419,17 @@ int batch_resident_ctas(const BatchGroupKey& g, int parity) {
     return max(1, sms * max(1, per_sm));
 }
 
+void conc_layout(ConcArgs& a) {
+    const long long nxy = (long long)a.F.nx * a.F.ny;
+    a.plane_blocks = (int)((nxy + kTile - 1) / kTile);
+    // a few planes per thread where the lattice gives enough CTAs without
+    a.zc = (int)std::min<long long>(8, std::max<long long>(1, (long long)a.F.nz * a.plane_blocks / 1024));
+}
+
+int conc_blocks(const ConcArgs& a) { return a.plane_blocks * ((a.F.nz + a.zc - 1) / a.zc); }
+
 cudaError_t launch_conv_diff(const ConcArgs& a, cudaStream_t s) {
-    dim3 grid((unsigned)((a.F.N + kTile - 1) / kTile)), block(kTile);
+    dim3 grid((unsigned)a.plane_blocks, (unsigned)((a.F.nz + a.zc - 1) / a.zc)), block(kTile);
     if (a.F.det_spread)
         conv_diff_kernel<true><<<grid, block, 0, s>>>(a);
     else

@@ -42,7 +42,14 @@ struct ConcArgs {
     int cur;        // index of the current concentration buffer
     int bump_iter;  // advance Ctl::iter (graph mode)
     FastDiv div_nx, div_nxy;
+    int plane_blocks;  // CTAs across an xy plane (kTile cells each)
+    int zc;            // planes each thread marches through
 };
+
+// plane_blocks and zc of a fluid's advection launch (conc_layout), and the
+// launch's CTA count
+void conc_layout(ConcArgs& a);
+int conc_blocks(const ConcArgs& a);
 
 // one system of a batch (device array, written when the batch changes)
 struct BatchSys {
