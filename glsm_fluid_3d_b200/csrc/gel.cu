@@ -515,8 +515,9 @@ __device__ void gel_run(const GelArgs& a, int gel_index, int* s_box, double* sta
             terms(G, I, geom_stage(G, stage));
             __syncthreads();
         }
+        // no barrier: nothing after it in this launch reads the Robin fields it
+        // clears, and the chemistry's element loads overlap its node stores
         set_zero(G, I);
-        __syncthreads();
     }
     if ((a.phases & kPhChem) && active) {
         chemistry(G, I);
