@@ -194,6 +194,21 @@ class Gel:
         fid = GEL_FIELDS[field] if isinstance(field, str) else int(field)
         check(self.L.glsm_gel_read(self.h, fid, _dptr(buf), buf.size), f"read {field}")
 
+    def snapshot(self, fields, bufs):
+        """Output snapshot (glsm_gel_snapshot): the fields as they are behind the
+        queued work go to the float64 buffers (page-locked, one per field, left
+        untouched until snapshot_wait) on a copy stream; returns at once."""
+        ids = (ctypes.c_int * len(fields))(*[GEL_FIELDS[f] if isinstance(f, str) else int(f) for f in fields])
+        for f, b in zip(fields, bufs):
+            fid = GEL_FIELDS[f] if isinstance(f, str) else int(f)
+            if b.dtype != np.float64 or not b.flags.c_contiguous or b.size != self.L.glsm_gel_field_size(self.h, fid):
+                raise ValueError(f"snapshot buffer for {f}: contiguous float64 of the field's size")
+        ptrs = (ctypes.POINTER(ctypes.c_double) * len(bufs))(*[_dptr(b) for b in bufs])
+        check(self.L.glsm_gel_snapshot(self.h, len(fields), ids, ptrs), "snapshot")
+
+    def snapshot_wait(self):
+        check(self.L.glsm_gel_snapshot_wait(self.h), "snapshot_wait")
+
     def write(self, field, values):
         fid = GEL_FIELDS[field] if isinstance(field, str) else int(field)
         v = np.ascontiguousarray(values, dtype=np.float64).ravel()
@@ -386,6 +401,17 @@ class Fluid:
     def read_into(self, field, buf):
         fid = FLUID_FIELDS[field] if isinstance(field, str) else int(field)
         check(self.L.glsm_fluid_read(self.h, fid, _fptr(buf), buf.size), f"read {field}")
+
+    def snapshot(self, u_buf, c_buf):
+        """Output snapshot (glsm_fluid_snapshot): u (3 N float32) and the current
+        c1 (N float32) behind the queued work, transferred to the page-locked
+        buffers on a copy stream; returns at once (see snapshot_wait)."""
+        if u_buf.dtype != np.float32 or c_buf.dtype != np.float32 or u_buf.size != 3 * self.N or c_buf.size != self.N:
+            raise ValueError("snapshot buffers: float32, 3 N and N values")
+        check(self.L.glsm_fluid_snapshot(self.h, _fptr(u_buf), _fptr(c_buf)), "snapshot")
+
+    def snapshot_wait(self):
+        check(self.L.glsm_fluid_snapshot_wait(self.h), "snapshot_wait")
 
     def write(self, field, values):
         fid = FLUID_FIELDS[field] if isinstance(field, str) else int(field)

@@ -51,6 +51,8 @@ def lib():
         "glsm_gel_add_noise": [vp, u64, d],
         "glsm_gel_read": [vp, i, P(d), ctypes.c_size_t],
         "glsm_gel_write": [vp, i, P(d), ctypes.c_size_t],
+        "glsm_gel_snapshot": [vp, i, P(i), P(P(d))],
+        "glsm_gel_snapshot_wait": [vp],
         "glsm_coupler_create": [P(vp), i, P(vp)],
         "glsm_coupler_destroy": [vp],
         "glsm_coupler_pack": [vp],
@@ -66,6 +68,8 @@ def lib():
         "glsm_fluid_run": [vp, i, i],
         "glsm_fluid_sync": [vp],
         "glsm_fluid_read": [vp, i, P(f), ctypes.c_size_t],
+        "glsm_fluid_snapshot": [vp, P(f), P(f)],
+        "glsm_fluid_snapshot_wait": [vp],
         "glsm_fluid_write": [vp, i, P(f), ctypes.c_size_t],
         "glsm_fluid_info": [vp, P(ctypes.c_int64)],
         "glsm_fluid_units": [vp, P(f)],
