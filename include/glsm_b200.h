@@ -166,7 +166,9 @@ int glsm_gel_add_noise(glsm_gel g, uint64_t seed, double amplitude);
 int glsm_gel_read(glsm_gel g, int field, double* dst, size_t count);
 int glsm_gel_write(glsm_gel g, int field, const double* src, size_t count);
 size_t glsm_gel_field_size(glsm_gel g, int field);
-/* device pointer of a field: the reference's public m_d* members */
+/* device pointer of a field: the reference's public m_d* members.  From then on
+ * glsm_fluid_run packs this gel's markers afresh at the start of every call, so
+ * writes through the pointer between calls reach the markers. */
 void* glsm_gel_device_ptr(glsm_gel g, int field);
 /* calFilamentD (src/gel_kernels.cu:837-866, run by Gel::recordCenter,
  * src/gel.cu:706-713): the points where the nodal u_norm and v_norm fields both
@@ -209,7 +211,10 @@ int glsm_fluid_step_velocity(glsm_fluid f, int iter);
 int glsm_fluid_step_concentration(glsm_fluid f, int iter);
 /* n whole coupled iterations iter0 .. iter0+n-1 in the order of src/sim.cpp:97-112
  * (gels, pack, stepVelocity, stepConcentration, repulsion, scatter), each one a
- * CUDA graph launch; asynchronous on the system stream */
+ * CUDA graph launch; asynchronous on the system stream.  The pack runs when the
+ * markers can have changed: after a gel's mechanics moved its nodes, and first in
+ * a call after a gel was changed through this interface or has a device pointer
+ * out (glsm_gel_device_ptr); it gives the same markers as packing every time. */
 int glsm_fluid_run(glsm_fluid f, int iter0, int n);
 /* wait for the system stream and report device-side error flags */
 int glsm_fluid_sync(glsm_fluid f);
