@@ -1721,10 +1721,12 @@ static int batch_rebuild(glsm_batch_s* b) {
             hm[2 * i + cb] = MarkerArgs{c->d_gels, c->mk, f->F.c[cb], f->F.source, f->F.nx, f->F.ny, f->F.nz, f->F.h, 1,
                                         f->F.det_spread};
         hr[i] = RepulsionArgs{c->d_gels, c->mk, c->rep_delta, c->rep_gamma, 1, nullptr, (int)c->gels.size(), f->F.h};
-        const int phases = kPhElastic | kPhChem | kPhRecord | kPhGather | kPhAuto;
+        // markers packed only when they can have changed, as in glsm_fluid_run
+        const int phases = kPhElastic | kPhChem | kPhRecord | kPhGather | kPhAuto | kPhGatherStale;
         for (int g = 0; g < (int)c->gels.size(); g++) {
             GelArgs ga = coupler_gel_args(c, phases, -1);
             ga.first_gel = g;
+            ga.gather_fresh = c->d_fresh;
             hg.push_back(ga);
         }
         conv_off[i + 1] = conv_off[i] + conc_blocks(hs[i].conc);
@@ -1894,6 +1896,7 @@ int glsm_batch_add(glsm_batch b, glsm_fluid f, int iter0, int n_iters) {
     set_iter_kernel<<<1, 1, 0, b->stream>>>(f->c->d_ctl, iter0);
     CK(cudaGetLastError());
     f->dev_iter = -1;  // the batch advances the counter
+    f->c->markers_stale = true;
     f->batch = b;
     b->sys.push_back(f);
     b->remaining.push_back(n_iters > 0 ? n_iters : -1);
@@ -1922,6 +1925,15 @@ int glsm_batch_run(glsm_batch b, int n) {
         if (r) return r;
     }
     if (b->sys.empty() || n == 0) return GLSM_OK;
+    for (glsm_fluid_s* f : b->sys) {
+        glsm_coupler c = f->c;
+        bool stale = c->markers_stale;
+        for (glsm_gel_s* g : c->gels) stale |= g->ptr_out;
+        if (stale && !c->gels.empty()) {
+            CK(cudaMemsetAsync(c->d_fresh, 0, sizeof(int) * c->gels.size(), b->stream));
+            c->markers_stale = false;
+        }
+    }
     for (int it = 0; it < n; it++) {
         CK(cudaGraphLaunch(b->graph[b->phase], b->stream));
         if (b->graph[1]) b->phase ^= 1;

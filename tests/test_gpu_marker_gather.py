@@ -132,3 +132,26 @@ def test_checkpoint_load_reaches_the_markers(gpu):
     assert np.array_equal(_lag(sim), _lag(ref))
     sim.close()
     ref.close()
+
+
+def test_batch_member_sees_node_changes_between_runs(gpu):
+    """The batched gel kernel packs markers by the same rule: a field write to a
+    member between batch runs reaches its markers at the next iteration."""
+    from glsm_fluid_3d_b200 import Batch
+
+    sim = _system("single")
+    b = Batch()
+    b.add(sim.fluid, 0, 0)
+    b.run(3)
+    b.sync()
+    before = _lag(sim).copy()
+    _host_write(sim)
+    b.run(1)  # iteration 3: no mechanics
+    b.sync()
+    d = _lag(sim) - before
+    b.remove(sim.fluid)
+    b.close()
+    sim.close()
+    assert np.allclose(d[:, 0], SHIFT, atol=4e-6), (d[:, 0].min(), d[:, 0].max())
+    assert np.abs(d[:, 1:]).max() == 0.0
+
