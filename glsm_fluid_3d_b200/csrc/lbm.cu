@@ -584,7 +584,10 @@ __device__ __forceinline__ void collide_scatter(const StepArgs& a, unsigned i, u
             const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
             const unsigned nbr = i + (unsigned)(cx + cy * (int)nx + cz * (int)nxy);
             if (cx == 0) {
-                IO::st_raw(P + (q * S + nbr), d[q]);
+                if (TAB)
+                    IO::st_raw(reinterpret_cast<T*>(a.scatter[q]) + i, d[q]);
+                else
+                    IO::st_raw(P + (q * S + nbr), d[q]);
             } else {
                 const bool edge = (cx > 0) ? (x == nx - 1) : (x == 0);
                 if (PERX)
@@ -674,7 +677,8 @@ __device__ __forceinline__ void lbm_cell(const StepArgs& a, unsigned i, bool inb
             const int cx = qcx(q), cy = qcy(q), cz = qcz(q);
             const long long off = cx + cy * Lnx + cz * Lnxy;
             if (cx == 0) {
-                d[q] = IO::raw(Pi + (qopp(q) * LS - off));
+                // no x wall in the way: the launch's table holds the address
+                d[q] = TAB ? IO::raw(reinterpret_cast<const T*>(a.gather[q]) + i) : IO::raw(Pi + (qopp(q) * LS - off));
             } else {
                 // across an x wall: the bounced opp(q) population of x, in slot q
                 // at x; periodic x: the wrapped neighbour
