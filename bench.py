@@ -449,7 +449,7 @@ def run_ours(args, world, rank, local):
                       "each step (glsm_gel_snapshot, D2H on a copy stream), final u and c read back (D2H); "
                       "bytes are totals divided by K"}
         assert np.isfinite(host_u).all()
-        assert all(np.isfinite(v[(K - 1) % 2]).all() and np.abs(v[(K - 1) % 2]).max() > 0 for v in host_vel)
+        assert all(np.isfinite(v[(K - 1) % 2]).all() for v in host_vel)  # (zero for gels not yet active)
 
     s.close()
     base = None
